@@ -1,0 +1,205 @@
+/*
+ * velo_b200.h — C ABI of the B200-native HLT1 VELO reconstruction chain.
+ *
+ * The chain replaces the VELO stage of LHCb Allen (Qwicen/cuda_hlt): the algorithms
+ *   init_event_list            cuda/global_event_cut/src/InitEventList.cu:7
+ *   estimate_input_size        cuda/velo/mask_clustering/src/EstimateInputSize.cu:3
+ *   prefix_sum_velo_clusters   cuda/utils/prefix_sum/include/PrefixSumHandler.cuh:270
+ *   masked_velo_clustering     cuda/velo/mask_clustering/src/MaskedVeloClustering.cu:48
+ *   calculate_phi_and_sort     cuda/velo/calculate_phi_and_sort/src/CalculatePhiAndSort.cu:6
+ *   fill_candidates            cuda/velo/search_by_triplet/src/FillCandidates.cu:72
+ *   search_by_triplet          cuda/velo/search_by_triplet/src/SearchByTriplet.cu:7
+ *   weak_tracks_adder          cuda/velo/search_by_triplet/src/WeakTracksAdder.cu:117
+ *   copy_and_prefix_sum_single_block_velo / copy_velo_track_hit_number /
+ *   prefix_sum_velo_track_hit_number
+ *                              cuda/utils/prefix_sum/src/PrefixSumSingleBlock.cu:130-168
+ *   consolidate_velo_tracks    cuda/velo/consolidate_tracks/src/ConsolidateVelo.cu:116
+ *   velo_kalman_fit            cuda/velo/simplified_kalman_filter/src/VeloKalmanFilter.cu:43
+ * as sequenced in configuration/sequences/Velo.h:5-18 (+ velo_kalman_fit_t from
+ * DefaultSequence.h:19). Inputs are the raw VP banks of RuntimeOptions
+ * (main/include/RuntimeOptions.h:9-55); outputs are the consolidated buffers of
+ * stream/setup/include/OutputArguments.cuh:16-34 in the layouts of
+ * cuda/event_model/common/include/ConsolidatedTypes.cuh:11-66 and
+ * cuda/event_model/velo/include/VeloConsolidated.cuh:12-144.
+ *
+ * Conventions: every entry point returns 0 or a negative VELO_ERR_* code and never throws.
+ * Device pointers are plain addresses; streams are cudaStream_t passed as void*. Nothing
+ * blocks except velo_sync. A context is used by one host thread at a time; separate
+ * contexts may run concurrently on separate streams.
+ */
+#ifndef VELO_B200_H
+#define VELO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- error codes (the reference throws instead: main/include/CudaCommon.h:10-18,
+ *      stream/gear/include/MemoryManager.cuh:78-80) ---- */
+#define VELO_OK 0
+#define VELO_ERR_INVALID -1      /* null pointer or bad argument */
+#define VELO_ERR_CUDA -2         /* a CUDA runtime call failed */
+#define VELO_ERR_CAPACITY -3     /* batch larger than the context was created for */
+#define VELO_ERR_BAD_RAW -4      /* malformed raw event */
+#define VELO_ERR_BAD_GEOMETRY -5 /* geometry blob has the wrong size */
+#define VELO_ERR_BAD_MC -6       /* malformed MC truth blob */
+#define VELO_ERR_NO_DEVICE -7    /* no CUDA device visible */
+#define VELO_ERR_STATE -8        /* call out of order (e.g. pruned run without weights) */
+
+/* ---- per-event status flags written by velo_run (status[N]) ---- */
+#define VELO_STATUS_BAD_RAW (1u << 0)
+#define VELO_STATUS_MODULE_OVERFLOW (1u << 1)
+#define VELO_STATUS_HIT_OVERFLOW (1u << 2)
+#define VELO_STATUS_CANDIDATE_OVERFLOW (1u << 3)
+#define VELO_STATUS_TRACK_OVERFLOW (1u << 4)
+#define VELO_STATUS_TTF_OVERFLOW (1u << 5)
+#define VELO_STATUS_WEAK_OVERFLOW (1u << 6)
+#define VELO_STATUS_H1_OVERFLOW (1u << 7)
+#define VELO_STATUS_BIG_SP_INDEX (1u << 8)
+#define VELO_STATUS_MLP_FALLBACK (1u << 9)
+
+/* ======================================================================
+ * Host utilities (libvelo_host.so; no GPU needed)
+ * ====================================================================== */
+
+/* SuperPixel pattern tables (same contents as cache_sp_patterns,
+ * x86/velo/clustering/src/ClusteringCommon.cpp:3-101; uploaded to the device by
+ * Constants::initialize_constants, stream/sequence/src/Constants.cu:45-53).
+ * patterns[256], sizes[256], fx[512], fy[512]. */
+void velo_build_sp_luts(uint8_t* patterns, uint8_t* sizes, float* fx, float* fy);
+
+/* Checks one raw event in the layout of cuda/velo/readme.md (the reader-side check is
+ * main/src/CheckVP.cpp:5-51). Returns 0 or VELO_ERR_BAD_RAW. */
+int velo_validate_raw_event(const void* event, uint64_t event_bytes);
+
+/* Seeded synthetic events: straight tracks from Poisson primary vertices through the real
+ * VELO geometry, encoded as SuperPixel raw banks, with MC truth in the MC_info layout of
+ * checker/tracking/src/MCEvent.cpp:16-92. Event i depends only on (seed, i). */
+typedef struct VeloGenConfig {
+  uint64_t seed;
+  float nu_min, nu_max;         /* pileup per event, uniform in [nu_min, nu_max] */
+  float visible_fraction;       /* primary vertices ~ Poisson(nu * visible_fraction) */
+  float tracks_per_pv;          /* charged tracks per vertex ~ Poisson(tracks_per_pv) */
+  float backward_fraction;      /* eta ~ U(-4,-2) with this probability, else U(2,5) */
+  float pv_sigma_xy, pv_sigma_z;/* mm */
+  float hit_efficiency;         /* per sensor crossing */
+  float p_one_pixel, p_two_pixels; /* cluster size 1/2/3 pixel probabilities (rest = 3) */
+  float noise_per_asic_per_nu;  /* random pixels per 256x256 ASIC ~ Poisson(this * nu) */
+  float noisy_event_fraction;   /* events with noise scaled by noisy_factor */
+  float noisy_factor;
+} VeloGenConfig;
+typedef struct VeloGenBatch VeloGenBatch;
+void velo_gen_default_config(VeloGenConfig* cfg);
+int velo_gen_create(const VeloGenConfig* cfg, const void* geometry, uint64_t first_event, uint32_t n_events,
+                    int n_threads, VeloGenBatch** out);
+uint64_t velo_gen_raw_bytes(const VeloGenBatch* b);
+uint64_t velo_gen_mc_bytes(const VeloGenBatch* b);
+/* raw_offsets / mc_offsets: n_events+1 byte offsets. truth_clusters: n_events (deposits). */
+int velo_gen_copy(const VeloGenBatch* b, void* raw, uint64_t* raw_offsets, void* mc, uint64_t* mc_offsets,
+                  uint32_t* truth_clusters);
+void velo_gen_destroy(VeloGenBatch* b);
+
+/* MC-truth checker for consolidated VELO tracks: the matching of
+ * checker/tracking/src/TrackChecker.cpp:349-405 and checker/tracking/include/MCAssociator.h:166-182
+ * (ghost = no MCP with weight >= 0.7), categories "Not electron long eta25"
+ * (checker/tracking/src/CategoriesTrackChecker.cpp:120) and "Not electron Velo" (:215). */
+typedef struct VeloCheckResult {
+  uint64_t events, tracks, ghosts;
+  uint64_t long_reconstructible, long_found, long_clones;
+  uint64_t velo_reconstructible, velo_found, velo_clones;
+  double long_efficiency, velo_efficiency, ghost_rate, ghost_rate_per_event;
+} VeloCheckResult;
+int velo_check_tracks(const void* mc_blob, const uint64_t* mc_offsets, uint32_t n_events,
+                      const uint32_t* event_track_offsets, const uint32_t* track_hit_offsets, const uint32_t* hit_ids,
+                      VeloCheckResult* res);
+
+/* ======================================================================
+ * GPU chain (libvelo_b200.so)
+ * ====================================================================== */
+typedef struct VeloCtx VeloCtx;
+
+#define VELO_MODE_PLAIN 0  /* exhaustive search_by_triplet (reference semantics) */
+#define VELO_MODE_PRUNED 1 /* learned seed/extension scorer prunes the search */
+
+#define VELO_MAP_AUTO 0    /* autotuned per hit-count bucket */
+#define VELO_MAP_BLOCK 1   /* decode/cluster/sort: one block per event */
+#define VELO_MAP_WARP 2    /* decode/cluster/sort: one warp per event */
+
+typedef struct VeloConfig {
+  uint32_t max_events;          /* events per velo_run call */
+  uint64_t max_raw_bytes;       /* raw input bytes per call */
+  uint32_t max_tracks;          /* consolidated tracks per call (0: 400 per event) */
+  uint32_t max_track_hits;      /* consolidated track hits per call (0: 16 per track) */
+  int32_t device;               /* CUDA device ordinal */
+  uint32_t mode;                /* VELO_MODE_* */
+  uint32_t mapping;             /* VELO_MAP_* */
+  uint32_t use_graphs;          /* capture the launch sequence in CUDA graphs per bucket */
+} VeloConfig;
+
+/* Output buffers of one velo_run call: device pointers, valid until the next velo_run on
+ * the same context. Layouts are the reference's:
+ *   atomics[2N+1]        tracks per event [0,N), exclusive offsets [N,2N], T = atomics[2N]
+ *   track_hit_number[T+1] exclusive scan of hits per track, H = track_hit_number[T]
+ *   track_hits           Velo::Consolidated::Hits SoA: float x[H], y[H], z[H], u32 LHCbID[H]
+ *   states / kalman_states Velo::Consolidated::States SoA over T: float x,y,tx,ty,c00,c20,c22,
+ *                        c11,c31,c33,chi2,z [T] each, then bool backward[T]
+ * Cluster container after the phi sort (for parity checks and downstream use):
+ *   module_hit_start[N*52], module_hit_num[N*52] (starts are absolute indices; gaps allowed),
+ *   hit_x/y/z/phi/id indexed by those starts. */
+typedef struct VeloOutputs {
+  uint32_t n_events;
+  uint32_t* atomics;
+  uint32_t* track_hit_number;
+  char* track_hits;
+  char* states;
+  char* kalman_states;
+  uint32_t* status;
+  uint32_t* module_hit_start;
+  uint32_t* module_hit_num;
+  float* hit_x;
+  float* hit_y;
+  float* hit_z;
+  float* hit_phi;
+  uint32_t* hit_id;
+  uint64_t hit_capacity;
+} VeloOutputs;
+
+/* Creates a context: device buffers for cfg->max_events events, device constants from the
+ * 19456-byte geometry blob (cuda/velo/common/src/ClusteringDefinitions.cu:23-53). */
+int velo_create(const VeloConfig* cfg, const void* geometry, size_t geometry_bytes, VeloCtx** out);
+
+/* Runs the chain on n_events raw events already in device memory: raw (byte buffer) and
+ * raw_offsets[n_events+1] (u64 byte offsets of each event in raw). Asynchronous on stream. */
+int velo_run(VeloCtx* ctx, const void* raw, const uint64_t* raw_offsets, uint32_t n_events, void* stream,
+             VeloOutputs* out);
+
+/* Same, from host buffers (pinned for overlap): copies the input to the context's device
+ * buffers on the stream, then runs. */
+int velo_run_host(VeloCtx* ctx, const void* raw_host, const uint64_t* raw_offsets_host, uint32_t n_events,
+                  void* stream, VeloOutputs* out);
+
+/* Waits for the context's last run; fills totals (tracks, track hits, clusters). */
+int velo_sync(VeloCtx* ctx, uint32_t* total_tracks, uint32_t* total_track_hits, uint64_t* total_clusters);
+
+/* Loads the learned seed/extension scorer (see velo_mlp_*); required for VELO_MODE_PRUNED. */
+int velo_set_mlp(VeloCtx* ctx, const void* weights_host, size_t bytes);
+
+/* Device time of each stage of the last run, milliseconds (decode+cluster+sort, search,
+ * scan, consolidate+fit); filled after velo_sync when timing was enabled. */
+int velo_stage_times(VeloCtx* ctx, float* ms, int n);
+int velo_set_timing(VeloCtx* ctx, int enabled);
+
+int velo_destroy(VeloCtx* ctx);
+
+/* Kernel launch count of the last run (all kernels of this library). */
+int velo_last_launch_count(VeloCtx* ctx, uint32_t* n);
+
+const char* velo_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VELO_B200_H */
