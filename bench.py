@@ -1,0 +1,471 @@
+#!/usr/bin/env python
+"""Throughput of the B200 VELO chain on the 500,000-event nu ~ U(2,15) workload.
+
+python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one pass of the chain over the rank's 500,000 synthetic events (seed 0,
+events rank*500000 ...), in batches of 16,384 events (one CUDA graph per batch).
+Events are independent, so ranks process disjoint event ranges with no data-path
+collective (weak scaling); NCCL is used only for the barrier and the max over ranks of
+the elapsed device time. Prints one JSON line (rank 0).
+  value   events/s with the raw banks resident in HBM (CUDA events around K steps)
+  e2e     events/s through velo_run_host from pinned host memory, each batch's
+          consolidated tracks and Kalman states read back to pinned host memory
+  roofline, cpu_baseline, clocks, gpu_launches: see DESIGN.md
+--impl reference times the CPU implementation of the chain (the CPU oracle restating the
+reference kernels; the reference has no CPU tracking) on the host cores, on a bounded
+sample of the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from cuda_hlt_b200 import chain, events  # noqa: E402
+
+METRIC = "VELO events/s on 1 B200, MLP-pruned vs plain at ≤0.2% eff loss; % HBM peak"
+UNIT = "events/s"
+WORKLOAD = "batched_500k"
+N_EVENTS = 500_000
+BUCKET = 16384
+CHUNK = 4 * BUCKET
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ---------------------------------------------------------------------------
+# clocks sampling during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
+             "clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, device_index):
+        self.device_index = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.reader = threading.Thread(target=self._read, daemon=True)
+            self.reader.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.reader.join(timeout=2)
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------
+def generate_workload(first_event, n_events, threads):
+    """Returns a list of EventBatch chunks (CHUNK events each, last one shorter)."""
+    chunks = []
+    for a in range(0, n_events, CHUNK):
+        n = min(CHUNK, n_events - a)
+        chunks.append(events.generate_config(WORKLOAD, n_events=n, first_event=first_event + a, threads=threads,
+                                             with_mc=False))
+    return chunks
+
+
+def batch_plan(chunks):
+    """Batches of at most BUCKET events inside each chunk: (chunk index, first, last)."""
+    plan = []
+    for ci, c in enumerate(chunks):
+        for a in range(0, c.n_events, BUCKET):
+            plan.append((ci, a, min(c.n_events, a + BUCKET)))
+    return plan
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def load_traffic():
+    """DRAM bytes per event of each kernel from the committed ncu summary, if present."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    threads = max(1, (os.cpu_count() or 1) // max(1, world))
+    t0 = time.time()
+    n_events = args.events
+    chunks = generate_workload(rank * n_events, n_events, threads)
+    log(f"[rank {rank}] generated {n_events} events in {time.time() - t0:.1f}s, "
+        f"{sum(c.raw.size for c in chunks) / 1e9:.2f} GB raw")
+    plan = batch_plan(chunks)
+    max_batch_bytes = max(int(chunks[ci].offsets[b] - chunks[ci].offsets[a]) for ci, a, b in plan)
+
+    # device-resident copy of the raw banks and per-batch offset arrays
+    d_raw = [torch.from_numpy(c.raw).to(dev) for c in chunks]
+    offs_host = []
+    for ci, a, b in plan:
+        o = chunks[ci].offsets[a:b + 1]
+        offs_host.append((o - o[0]).astype(np.uint64))
+    d_offs = [torch.from_numpy(o.view(np.int64)).to(dev) for o in offs_host]
+    batch_ptrs = [(d_raw[ci].data_ptr() + int(chunks[ci].offsets[a]), d_offs[k].data_ptr(), b - a)
+                  for k, (ci, a, b) in enumerate(plan)]
+    stream = torch.cuda.current_stream(dev).cuda_stream
+
+    vc = chain.VeloChain(max_events=BUCKET, max_raw_bytes=max_batch_bytes + 4096, device=local_rank,
+                         use_graphs=True)
+    vc.set_timing(True)
+
+    # census: per-batch totals for the algorithmic-byte accounting
+    clusters = tracks = track_hits = 0
+    for raw_p, off_p, n in batch_ptrs:
+        vc.run_device(raw_p, off_p, n, stream)
+        t, h, c = vc.sync()
+        tracks += t
+        track_hits += h
+        clusters += c
+    raw_bytes = sum(int(c.raw.size) for c in chunks)
+
+    def step():
+        for raw_p, off_p, n in batch_ptrs:
+            vc.run_device(raw_p, off_p, n, stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    vc.set_timing(True)  # keep only the timed region's event records
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clocks:
+        start.record()
+        for _ in range(args.steps):
+            step()
+        end.record()
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    elapsed_ms = start.elapsed_time(end)
+    if world > 1:
+        t = torch.tensor([elapsed_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+    stages = vc.stage_times()
+    n_batches = len(plan)
+    value = n_events * world * args.steps / (elapsed_ms / 1e3)
+    ms_per_step = elapsed_ms / args.steps
+
+    # ---- roofline of the dominant kernel (per launch = one batch) ----
+    per = {  # algorithmic bytes of one step, per stage
+        "decode_cluster_sort": raw_bytes + 16 * clusters,
+        "search_by_triplet": 16 * clusters + 2 * track_hits + 2 * tracks,
+        "event_scan": 16 * n_events,
+        "consolidate_fit": 34 * track_hits + 98 * tracks + 8 * tracks,
+    }
+    stage_ms = {k: stages[k] for k in chain.STAGES}
+    dominant = max(stage_ms, key=stage_ms.get)
+    avg_launch_ms = stage_ms[dominant] / max(1, stages["runs"])
+    alg_bytes_launch = per[dominant] / n_batches
+    achieved = alg_bytes_launch / (avg_launch_ms / 1e3) / 1e9
+    peak, peak_kind = load_peaks()
+    traffic = None
+    tr = load_traffic()
+    if tr and dominant in tr.get("bytes_per_event", {}):
+        traffic = tr["bytes_per_event"][dominant] * n_events / n_batches
+
+    # ---- end to end through velo_run_host with host buffers ----
+    e2e = run_e2e(args, chunks, plan, local_rank, torch, world, dist)
+
+    result = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+        "config": {"workload": f"{WORKLOAD}: {n_events} events per GPU, pileup nu ~ U(2,15), seed 0, "
+                               f"events rank*{n_events}...", "events_per_gpu": n_events, "batch_events": BUCKET,
+                   "batches_per_step": n_batches, "mode": "plain", "graphs": True,
+                   "l2": f"inputs larger than L2 ({raw_bytes / 1e9:.2f} GB raw banks per step)",
+                   "parallelism": f"event shards x{world}"},
+        "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "peak_source": peak_kind,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": alg_bytes_launch, "avg_launch_ms": avg_launch_ms,
+                     "chain_alg_bytes_per_event": (raw_bytes + 16 * track_hits + 98 * tracks + 4 * (tracks + n_batches)
+                                                   + 8 * n_batches) / n_events},
+        "stages_ms_per_step": stage_ms,
+        "totals_per_step": {"clusters": clusters, "tracks": tracks, "track_hits": track_hits, "raw_bytes": raw_bytes},
+        "e2e": e2e,
+        "gpu_launches": 4 * n_batches * args.steps,
+        "clocks": clocks.summary(),
+    }
+    vc.close()
+    return result, chunks
+
+
+def run_e2e(args, chunks, plan, local_rank, torch, world, dist):
+    """velo_run_host from pinned memory, two contexts alternating on two streams so that
+    the copies of one batch overlap the kernels of the other; outputs read back to pinned
+    host buffers every batch."""
+    import ctypes as C
+    cudart = torch.cuda.cudart()
+    for c in chunks:
+        cudart.cudaHostRegister(c.raw.ctypes.data, c.raw.nbytes, 0)
+    offs = []
+    for ci, a, b in plan:
+        o = chunks[ci].offsets[a:b + 1]
+        offs.append(np.ascontiguousarray(o - o[0], dtype=np.uint64))
+    max_batch_bytes = max(int(chunks[ci].offsets[b] - chunks[ci].offsets[a]) for ci, a, b in plan)
+    ctxs = [chain.VeloChain(max_events=BUCKET, max_raw_bytes=max_batch_bytes + 4096, device=local_rank)
+            for _ in range(2)]
+    streams = [torch.cuda.Stream(device=local_rank) for _ in range(2)]
+    # pinned result buffers per context: atomics, hit numbers, hits SoA, Kalman states
+    cap_t = 400 * BUCKET
+    cap_h = 16 * cap_t
+    outs = [dict(atomics=torch.empty(2 * BUCKET + 1, dtype=torch.int32, pin_memory=True),
+                 thn=torch.empty(cap_t + 1, dtype=torch.int32, pin_memory=True),
+                 hits=torch.empty(16 * cap_h, dtype=torch.uint8, pin_memory=True),
+                 kal=torch.empty(52 * cap_t, dtype=torch.uint8, pin_memory=True)) for _ in range(2)]
+    lib = ctxs[0].lib
+
+    d2h = [0]
+    h2d = [0]
+
+    def fetch(k):
+        vc, o, s = ctxs[k % 2], outs[k % 2], streams[k % 2]
+        t, h, _ = vc.sync(clusters=False)
+        n = plan[k][2] - plan[k][1]
+        for buf, src, nbytes in ((o["atomics"], vc.out.atomics, 4 * (2 * n + 1)),
+                                 (o["thn"], vc.out.track_hit_number, 4 * (t + 1)),
+                                 (o["hits"], vc.out.track_hits, 16 * h),
+                                 (o["kal"], vc.out.kalman_states, 49 * t)):
+            if nbytes:
+                chain._check(lib.velo_download_async(vc.ctx, C.c_void_p(buf.data_ptr()), C.c_void_p(src), nbytes,
+                                                     C.c_void_p(s.cuda_stream)), "velo_download_async")
+                d2h[0] += nbytes
+
+    def step():
+        pending = None
+        for k, (ci, a, b) in enumerate(plan):
+            vc, s = ctxs[k % 2], streams[k % 2]
+            base = int(chunks[ci].offsets[a])
+            nbytes = int(chunks[ci].offsets[b]) - base
+            sub = events.EventBatch(chunks[ci].raw[base:base + nbytes], offs[k])
+            vc.run_host(sub, s.cuda_stream)
+            h2d[0] += nbytes + offs[k].nbytes
+            if pending is not None:
+                fetch(pending)
+            pending = k
+        fetch(pending)
+        for s in streams:
+            s.synchronize()
+
+    for _ in range(max(1, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    d2h[0] = h2d[0] = 0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([el], device=torch.device("cuda", local_rank), dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        el = float(t.item())
+    for vc in ctxs:
+        vc.close()
+    for c in chunks:
+        cudart.cudaHostUnregister(c.raw.ctypes.data)
+    n_events = sum(b - a for _, a, b in plan)
+    return {"value": n_events * world * args.steps / el, "unit": UNIT,
+            "h2d_bytes_per_step": h2d[0] // args.steps, "d2h_bytes_per_step": d2h[0] // args.steps,
+            "timing": "host wall clock around K steps, synchronised"}
+
+
+# ---------------------------------------------------------------------------
+# CPU baselines
+# ---------------------------------------------------------------------------
+def cpu_baseline(sample_events, threads):
+    """The CPU oracle (restatement of the reference chain; the reference has no CPU
+    tracking) on a bounded sample, plus the reference's own x86 clustering when built."""
+    import oracle
+    geo = events.load_geometry()
+    b = events.generate_config(WORKLOAD, n_events=sample_events, threads=threads, with_mc=False)
+    t0 = time.perf_counter()
+    oracle.run(b, geo, threads=threads)
+    dt = time.perf_counter() - t0
+    out = {"value": sample_events / dt, "unit": UNIT, "cores": threads, "kind": "port",
+           "sample": f"first {sample_events} events of the workload, full chain, {threads} threads"}
+    if os.path.exists(oracle.REF_X86_LIB):
+        try:
+            t0 = time.perf_counter()
+            oracle.ref_x86_clustering(b, geo, algo=0, threads=threads)
+            out["reference_x86_clustering_only"] = {
+                "value": sample_events / (time.perf_counter() - t0), "unit": UNIT, "kind": "reference",
+                "what": "x86/velo/clustering clustering() only (the reference's only CPU VELO code)"}
+        except Exception as ex:  # pragma: no cover
+            out["reference_x86_clustering_only"] = {"error": str(ex)}
+    return out, b
+
+
+def reference_gpu(batch):
+    """The reference's own CUDA kernels (oracle/_ref) on one batch, visitor launch shapes
+    and host synchronisations included; events above its 500-cluster module buffer are
+    left out (they would overrun its shared memory)."""
+    import oracle
+    geo = events.load_geometry()
+    if not os.path.exists(oracle.REF_GPU_LIB):
+        return None
+    r = oracle.run(batch, geo)
+    # events that overrun the reference's fixed per-event buffers would spill into their
+    # neighbours; they are left out so that the reference run stays well defined
+    keep = [e for e in range(batch.n_events) if r.module_num[e * 52:(e + 1) * 52].max() < 500
+            and not (r.flags[e] & oracle.UNDEFINED_IN_REFERENCE & ~oracle.F_SEED_TIE)]
+    sub = events.EventBatch(np.concatenate([batch.event(e) for e in keep]),
+                            np.concatenate([[0], np.cumsum([batch.event(e).size for e in keep])]).astype(np.uint64))
+    _, ms = oracle.ref_gpu_run(sub, geo, reps=4)
+    return {"value": len(keep) / (ms / 1e3), "unit": UNIT, "events": len(keep),
+            "what": "reference cuda/velo kernels compiled for sm_100a, one batch per launch sequence"}
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the CPU implementation on the host cores
+# ---------------------------------------------------------------------------
+def run_reference(args):
+    import oracle
+    threads = os.cpu_count() or 1
+    geo = events.load_geometry()
+    sample = args.reference_sample
+    b = events.generate_config(WORKLOAD, n_events=sample, threads=threads, with_mc=False)
+    for _ in range(args.warmup):
+        oracle.run(b, geo, threads=threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        oracle.run(b, geo, threads=threads)
+        times.append(time.perf_counter() - t0)
+    value = sample * args.steps / sum(times)
+    return {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+        "config": {"workload": f"{WORKLOAD}: bounded sample of {sample} events per step (first events of the "
+                               f"500,000-event workload)", "mode": "plain"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{sample} events per step, full chain"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--events", type=int, default=N_EVENTS, help="events per GPU (default: the 500,000 workload)")
+    ap.add_argument("--cpu-sample", type=int, default=16384)
+    ap.add_argument("--reference-sample", type=int, default=8192)
+    ap.add_argument("--no-extras", action="store_true", help="skip the CPU baseline and reference-GPU legs")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        print(json.dumps(run_reference(args)), flush=True)
+        return 0
+
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    result, chunks = run_ours(args, rank, world, local_rank)
+    if rank == 0 and not args.no_extras:
+        threads = os.cpu_count() or 1
+        try:
+            result["cpu_baseline"], sample = cpu_baseline(min(args.cpu_sample, args.events), threads)
+        except Exception as ex:
+            result["cpu_baseline"] = {"error": str(ex)}
+            sample = None
+        if world == 1:
+            try:
+                b0 = chunks[0].subset(0, min(BUCKET, chunks[0].n_events))
+                result["reference_gpu_b200"] = reference_gpu(b0)
+            except Exception as ex:
+                result["reference_gpu_b200"] = {"error": str(ex)}
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -104,6 +104,8 @@ GPU_SYMBOLS = [
     "velo_stage_times",
     "velo_set_timing",
     "velo_destroy",
+    "velo_download",
+    "velo_download_async",
     "velo_last_launch_count",
     "velo_version",
 ]
@@ -165,6 +167,10 @@ def gpu_lib():
         lib.velo_set_timing.restype = C.c_int
         lib.velo_destroy.argtypes = [P]
         lib.velo_destroy.restype = C.c_int
+        lib.velo_download.argtypes = [P, P, P, C.c_size_t]
+        lib.velo_download.restype = C.c_int
+        lib.velo_download_async.argtypes = [P, P, P, C.c_size_t, P]
+        lib.velo_download_async.restype = C.c_int
         lib.velo_last_launch_count.argtypes = [P, C.POINTER(C.c_uint32)]
         lib.velo_last_launch_count.restype = C.c_int
         lib.velo_version.argtypes = []

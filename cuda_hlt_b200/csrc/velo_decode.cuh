@@ -1,0 +1,467 @@
+// Kernel 1 of the chain: SuperPixel decode, masked clustering, phi and per-module sort.
+//
+// One block per event (persistent; events are pulled from a device queue). Work is flat
+// over the event's SP words: each thread takes SPs, finds the neighbouring SPs it needs by
+// binary search in the bank (banks are address-sorted in LHCb raw data; unsorted banks
+// fall back to the reference's linear scan, with the same result), clusters, and appends
+// the clusters to its module's slice of the event's hit region. The module slices are
+// then sorted in place on (phi, LHCb id) by one warp each (bitonic network in shared
+// memory). The result equals the reference's estimate -> prefix sum -> masked clustering
+// -> calculate_phi_and_sort sequence, whose slot order within a module is atomic-order
+// dependent only for exactly equal phi.
+#pragma once
+#include "velo_kernels.cuh"
+
+namespace velo {
+
+constexpr uint32_t kSortCap = 512;  // clusters per module sorted in shared memory
+
+// SPs around one SP: the non-isolated ones of the 4x3-SP flood window
+// (MaskedVeloClustering.cu:221-272) and, over every SP of the bank, the five neighbours the
+// candidate search reads (EstimateInputSize.cu:124-153).
+struct SpWindow {
+  uint32_t px[3];
+  uint32_t top, top_right, right, right_bottom, bottom;
+};
+
+__device__ __forceinline__ void window_add(SpWindow& w, uint32_t o, int32_t r, int32_t c)
+{
+  const int32_t orow = sp_row(o), ocol = sp_col(o);
+  const uint32_t osp = sp_mask(o);
+  if (!sp_isolated(o) && orow >= r - 2 && orow <= r + 1 && ocol >= c - 1 && ocol <= c + 1) {
+    const int32_t rr = orow - (r - 2), rc = ocol - (c - 1);
+    w.px[rc] |= (osp & 0x0Fu) << (4 * rr) | (osp & 0xF0u) << (12 + 4 * rr);
+  }
+  if (ocol == c) {
+    if (orow == r + 1) w.top |= osp;
+    if (orow == r - 1) w.bottom |= osp;
+  } else if (ocol == c + 1) {
+    if (orow == r + 1) w.top_right |= osp;
+    if (orow == r) w.right |= osp;
+    if (orow == r - 1) w.right_bottom |= osp;
+  }
+}
+
+__device__ __forceinline__ uint32_t bank_lower_bound(const uint32_t* bank, uint32_t count, uint32_t addr)
+{
+  uint32_t lo = 0, hi = count;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (sp_addr(__ldg(bank + mid)) < addr) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ SpWindow gather_window(const uint32_t* bank, uint32_t count, bool sorted, int32_t r,
+                                                  int32_t c)
+{
+  SpWindow w{{0u, 0u, 0u}, 0u, 0u, 0u, 0u, 0u};
+  if (sorted) {
+    const int32_t rlo = max(r - 2, 0), rhi = min(r + 1, 63);
+#pragma unroll 1
+    for (int32_t col = max(c - 1, 0); col <= min(c + 1, 511); ++col) {
+      const uint32_t a_hi = (static_cast<uint32_t>(col) << 6) | rhi;
+      for (uint32_t i = bank_lower_bound(bank, count, (static_cast<uint32_t>(col) << 6) | rlo); i < count; ++i) {
+        const uint32_t o = __ldg(bank + i);
+        if (sp_addr(o) > a_hi) break;
+        window_add(w, o, r, c);
+      }
+    }
+  } else {
+    for (uint32_t i = 0; i < count; ++i) window_add(w, __ldg(bank + i), r, c);
+  }
+  return w;
+}
+
+// Candidate-pixel code of a non-isolated SP from its neighbours (EstimateInputSize.cu:118-183).
+__device__ __forceinline__ uint32_t window_candidate_code(uint32_t sp, const SpWindow& w)
+{
+  uint32_t pixels = (sp & 0x0Fu) | ((sp & 0xF0u) << 2);
+  pixels |= ((w.top & 0x01u) | ((w.top & 0x10u) << 2)) << 4;
+  pixels |= (w.top_right & 0x01u) << 16;
+  pixels |= (w.right & 0x0Fu) << 12;
+  pixels |= (w.right_bottom & 0x08u) << 8;
+  pixels |= (w.bottom & 0x80u) >> 2;
+  const uint32_t inside = pixels & 0x3CFu;
+  const uint32_t mask = (inside << 1) | (inside << 5) | (inside << 6) | (inside << 7);
+  const uint32_t open = mask & (~pixels);
+  const uint32_t cand = (open >> 1) & (open >> 5) & (open >> 6) & (open >> 7) & pixels;
+  return (cand & 0x03u) | ((cand & 0xC0u) >> 4) | ((cand & 0x0Cu) << 2) | ((cand & 0x0300u) >> 2);
+}
+
+// Flood fill seeded by pixel k of the SP at (sp_r, sp_c) over the window pixels
+// (MaskedVeloClustering.cu:274-398). True when the cluster is stored.
+__device__ __forceinline__ bool flood_window(uint32_t px0, uint32_t px1, uint32_t px2, int32_t sp_r, int32_t sp_c,
+                                             uint32_t k, int32_t& xs, int32_t& ys, int32_t& n)
+{
+  const int32_t row_lower_limit = (sp_r - 2) * 4, col_lower_limit = (sp_c - 1) * 2;
+  const uint32_t row = sp_r * 4 + (k % 4);
+  const uint32_t col = sp_c * 2 + (k >= 4);
+  const uint32_t seed = (0x01u << (row - row_lower_limit)) << (16 * (col % 2));
+  uint32_t cl0 = 0, cl1 = seed, cl2 = 0;
+  uint32_t w0 = 0, w1 = seed, w2 = 0;
+  px1 &= ~cl1;
+#pragma unroll 1
+  for (uint32_t it = 0; it < kMaxClusteringIterations; ++it) {
+    const uint32_t m0 = flood_mask(w0) | flood_right_to_left(w1);
+    const uint32_t m1 = flood_mask(w1) | flood_right_to_left(w2) | flood_left_to_right(w0);
+    const uint32_t m2 = flood_mask(w2) | flood_left_to_right(w1);
+    w0 = px0 & m0;
+    w1 = px1 & m1;
+    w2 = px2 & m2;
+    if ((w0 | w1 | w2) == 0u) break;
+    cl0 |= w0;
+    cl1 |= w1;
+    cl2 |= w2;
+    px0 &= ~cl0;
+    px1 &= ~cl1;
+    px2 &= ~cl2;
+  }
+  if (cl2) return false;  // a pixel in the SP column to the right owns this cluster
+  n = __popc(cl0) + __popc(cl1);
+  if (n >= 3) {
+    const uint32_t c0 = found_cluster_mask(cl0) & ~cl0;
+    const uint32_t c1 = (found_cluster_mask(cl1) | flood_left_to_right(cl0)) & ~cl1;
+    const uint32_t c2 = flood_left_to_right(cl1);
+    const uint32_t cand0 = precedence_candidates(c0, c1) & cl0;
+    const uint32_t cand1 = (precedence_candidates(c1, c2) & cl1) ^ seed;
+    if (cand0 | cand1) {
+      const int32_t neg = ~(-static_cast<int32_t>(seed));
+      const bool under = seed < 4096u;
+      uint32_t smaller_row = under * (0xFFF & neg) | (!under) * (0xFFF & (neg >> 16));
+      smaller_row |= smaller_row << 16;
+      const uint32_t current = smaller_row | under * 0xFFFF0000u;
+      if (((cand0 & smaller_row) | (cand1 & current)) != 0u) return false;
+    }
+  }
+  xs = __popc(cl0 & 0x0000FFFFu) * col_lower_limit + __popc(cl0 & 0xFFFF0000u) * (col_lower_limit + 1) +
+       __popc(cl1 & 0x0000FFFFu) * (col_lower_limit + 2) + __popc(cl1 & 0xFFFF0000u) * (col_lower_limit + 3);
+  const uint32_t t0 = (cl0 & 0x000F000Fu) | ((cl1 & 0x000F000Fu) << 4);
+  const uint32_t t1 = ((cl0 & 0x00F000F0u) >> 4) | (cl1 & 0x00F000F0u);
+  const uint32_t t2 = ((cl0 & 0x0F000F00u) >> 8) | ((cl1 & 0x0F000F00u) >> 4);
+  const uint32_t t3 = ((cl0 & 0xF000F000u) >> 12) | ((cl1 & 0xF000F000u) >> 8);
+  int32_t y = 0;
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const uint32_t m = 0x11111111u << r;
+    y += __popc(t0 & m) * (row_lower_limit + r) + __popc(t1 & m) * (row_lower_limit + 4 + r) +
+         __popc(t2 & m) * (row_lower_limit + 8 + r) + __popc(t3 & m) * (row_lower_limit + 12 + r);
+  }
+  ys = y;
+  return true;
+}
+
+struct DecodeShared {
+  uint32_t bank_start[kSensors];  // word index (from the event start) of the first SP word
+  uint32_t bank_count[kSensors];
+  uint32_t bank_sensor[kSensors];
+  uint32_t sp_prefix[kSensors + 1];  // exclusive scan of bank_count
+  uint32_t unsorted[(kSensors + 31) / 32];
+  uint32_t mod_count[kModules];
+  uint32_t mod_start[kModules];
+  uint32_t mod_fill[kModules];
+  uint32_t event;
+  uint32_t flags;
+  uint32_t n_candidates;
+};
+
+// Clusters of SP number f of the event (flat over banks). Returns the cluster count; with
+// emit, the clusters are placed into pts.
+template<bool emit>
+__device__ __forceinline__ uint32_t sp_clusters(const DecodeShared& sh, const uint32_t* ev, const ChainPointers& P,
+                                                const GeometryView& g, uint32_t f, uint32_t& bank_out,
+                                                uint32_t& cands, ClusterPoint* pts)
+{
+  // bank of flat index f: last b with sp_prefix[b] <= f
+  uint32_t lo = 0, hi = kSensors;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (sh.sp_prefix[mid] <= f) lo = mid; else hi = mid;
+  }
+  const uint32_t b = lo;
+  bank_out = b;
+  const uint32_t s = f - sh.sp_prefix[b];
+  const uint32_t* bank = ev + sh.bank_start[b];
+  const uint32_t count = sh.bank_count[b];
+  const uint32_t sensor = sh.bank_sensor[b];
+  const bool sorted = !((sh.unsorted[b >> 5] >> (b & 31)) & 1u);
+  const uint32_t word = __ldg(bank + s);
+  const uint32_t sp = sp_mask(word);
+  const int32_t sp_r = sp_row(word), sp_c = sp_col(word);
+  uint32_t n = 0;
+  cands = 0;
+  if (sp_isolated(word)) {
+    // isolated SP: pattern table (MaskedVeloClustering.cu:105-167)
+    const uint32_t idx = __ldg(P.k.sp_patterns + sp);
+    n = 1 + ((idx >> 3) & 1u);
+    if (emit) {
+      const uint32_t chip = sp_c / (kChipColumns / 2);
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        if (c == 1 && !(idx & 8)) break;
+        const uint32_t row = c ? (idx >> 4) & 3u : idx & 0x03u;
+        const uint32_t col = c ? (idx >> 6) & 1u : (idx >> 2) & 1u;
+        const uint32_t cx = sp_c * 2 + col;
+        const uint32_t cy = sp_r * 4 + row;
+        const float fx = __ldg(P.k.sp_fx + sp * 2 + c);
+        const float fy = __ldg(P.k.sp_fy + sp * 2 + c);
+        pts[c] = place_cluster(g, sensor, cx, cy, fx, fy, chip);
+      }
+    }
+    return n;
+  }
+  const SpWindow w = gather_window(bank, count, sorted, sp_r, sp_c);
+  const uint32_t code = window_candidate_code(sp, w);
+  if (!code) return 0;
+  // The reference packs the SP index into a u8 when it decodes candidates
+  // (MaskedVeloClustering.cu:179), so above 255 SPs the flood runs on SP s & 0xFF.
+  const uint32_t s2 = s & 0xFFu;
+  uint32_t px0 = w.px[0], px1 = w.px[1], px2 = w.px[2];
+  int32_t r2 = sp_r, c2 = sp_c;
+  if (s2 != s) {
+    const uint32_t word2 = __ldg(bank + s2);
+    r2 = sp_row(word2);
+    c2 = sp_col(word2);
+    const SpWindow w2 = gather_window(bank, count, sorted, r2, c2);
+    px0 = w2.px[0];
+    px1 = w2.px[1];
+    px2 = w2.px[2];
+  }
+#pragma unroll
+  for (int half = 0; half < 2; ++half) {
+    const uint32_t nib = half ? code >> 4 : code & 0xFu;
+    if (!nib) continue;
+    ++cands;
+    const uint32_t k = candidate_k(nib) + 2 * half;
+    int32_t xs, ys, np;
+    if (flood_window(px0, px1, px2, r2, c2, k, xs, ys, np)) {
+      if (emit) {
+        const uint32_t cx = xs / np;
+        const uint32_t cy = ys / np;
+        const float fx = xs / static_cast<float>(np) - cx;
+        const float fy = ys / static_cast<float>(np) - cy;
+        pts[n] = place_cluster(g, sensor, cx, cy, fx, fy, cx / kChipColumns);
+      }
+      ++n;
+    }
+  }
+  return n;
+}
+
+// Bitonic sort of (key, slot) pairs in shared memory by one warp; size is a power of two.
+__device__ __forceinline__ void warp_bitonic_sort(unsigned long long* key, uint16_t* slot, uint32_t size)
+{
+  const uint32_t lane = lane_id();
+  for (uint32_t k = 2; k <= size; k <<= 1) {
+    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+      for (uint32_t i = lane; i < size; i += 32) {
+        const uint32_t ixj = i ^ j;
+        if (ixj > i) {
+          const unsigned long long a = key[i], b = key[ixj];
+          const bool ascending = (i & k) == 0;
+          if ((a > b) == ascending) {
+            key[i] = b;
+            key[ixj] = a;
+            const uint16_t t = slot[i];
+            slot[i] = slot[ixj];
+            slot[ixj] = t;
+          }
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+template<int W>
+__global__ void __launch_bounds__(W * 32) decode_cluster_sort_kernel(ChainPointers P)
+{
+  __shared__ DecodeShared sh;
+  __shared__ unsigned long long s_key[W][kSortCap];
+  __shared__ uint16_t s_slot[W][kSortCap];
+  const uint32_t warp = threadIdx.x >> 5, lane = lane_id();
+  const GeometryView g = geometry_view(P.k.geometry);
+
+  for (;;) {
+    if (threadIdx.x == 0) {
+      sh.event = atomicAdd(P.queue + 0, 1u);
+      sh.flags = 0;
+      sh.n_candidates = 0;
+    }
+    if (threadIdx.x < (kSensors + 31) / 32) sh.unsorted[threadIdx.x] = 0;
+    if (threadIdx.x < kModules) sh.mod_fill[threadIdx.x] = 0;
+    __syncthreads();
+    const uint32_t e = sh.event;
+    if (e >= P.n_events) break;
+    const uint64_t off = P.raw_offsets[e];
+    const uint64_t bytes = P.raw_offsets[e + 1] - off;
+    const uint32_t* ev = reinterpret_cast<const uint32_t*>(P.raw + off);
+    const uint64_t words = bytes / 4;
+    const uint32_t header = 2 + kSensors;  // number_of_raw_banks + raw_bank_offset[209]
+    // ---- validate the raw event and index its banks ----
+    const bool bad_header = (off & 3) || words < header + 1 || __ldg(ev) != kSensors;
+    if (!bad_header) {
+      const uint64_t payload_bytes = (words - header) * 4;
+      for (uint32_t b = threadIdx.x; b < kSensors; b += blockDim.x) {
+        const uint32_t o = __ldg(ev + 1 + b), o1 = __ldg(ev + 2 + b);
+        bool ok = !(o & 3) && o1 >= o + 8 && o1 <= payload_bytes;
+        uint32_t sensor = 0, count = 0;
+        if (ok) {
+          sensor = __ldg(ev + header + o / 4);
+          count = __ldg(ev + header + o / 4 + 1);
+          ok = sensor == b && 8ull + 4ull * count <= static_cast<uint64_t>(o1 - o);
+        }
+        if (!ok) {
+          atomicOr(&sh.flags, kStatusBadRawEvent);
+          count = 0;
+        }
+        sh.bank_start[b] = header + o / 4 + 2;
+        sh.bank_count[b] = count;
+        sh.bank_sensor[b] = sensor;
+        if (count > 256) atomicOr(&sh.flags, kStatusBigSpIndex);
+      }
+    } else if (threadIdx.x == 0) {
+      atomicOr(&sh.flags, kStatusBadRawEvent);
+    }
+    __syncthreads();
+    const bool event_ok = !(sh.flags & kStatusBadRawEvent);
+    if (!event_ok)
+      for (uint32_t b = threadIdx.x; b <= kSensors; b += blockDim.x) sh.sp_prefix[b] = 0;
+    // ---- bank prefix (warp 0) and sortedness of each bank (all threads) ----
+    if (event_ok) {
+      if (warp == 0) {
+        uint32_t carry = 0;
+        for (uint32_t b0 = 0; b0 < kSensors; b0 += 32) {
+          const uint32_t b = b0 + lane;
+          const uint32_t v = b < kSensors ? sh.bank_count[b] : 0;
+          uint32_t incl = v;
+#pragma unroll
+          for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= static_cast<uint32_t>(o)) incl += t;
+          }
+          if (b < kSensors) sh.sp_prefix[b] = carry + incl - v;
+          carry += __shfl_sync(0xFFFFFFFFu, incl, 31);
+        }
+        if (lane == 0) sh.sp_prefix[kSensors] = carry;
+      }
+      for (uint32_t b = warp; b < kSensors; b += W) {
+        const uint32_t* bank = ev + sh.bank_start[b];
+        const uint32_t count = sh.bank_count[b];
+        bool unsorted = false;
+        for (uint32_t i = lane + 1; i < count; i += 32)
+          unsorted |= sp_addr(__ldg(bank + i)) < sp_addr(__ldg(bank + i - 1));
+        if (__any_sync(0xFFFFFFFFu, unsorted) && lane == 0) atomicOr(&sh.unsorted[b >> 5], 1u << (b & 31));
+      }
+    }
+    __syncthreads();
+    const uint32_t total_sp = sh.sp_prefix[kSensors];
+    // ---- count pass ----
+    if (threadIdx.x < kModules) sh.mod_count[threadIdx.x] = 0;
+    __syncthreads();
+    uint32_t my_cands = 0;
+    for (uint32_t f = threadIdx.x; f < total_sp; f += blockDim.x) {
+      uint32_t b, cands;
+      const uint32_t n = sp_clusters<false>(sh, ev, P, g, f, b, cands, nullptr);
+      if (n) atomicAdd(&sh.mod_count[b >> 2], n);
+      my_cands += cands;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) my_cands += __shfl_xor_sync(0xFFFFFFFFu, my_cands, o);
+    if (lane == 0 && my_cands) atomicAdd(&sh.n_candidates, my_cands);
+    __syncthreads();
+    if (warp == 0) {
+      const uint32_t a = lane < kModules ? sh.mod_count[lane] : 0;
+      const uint32_t a2 = lane + 32 < kModules ? sh.mod_count[lane + 32] : 0;
+      uint32_t ia = a, ib = a2;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t va = __shfl_up_sync(0xFFFFFFFFu, ia, o), vb = __shfl_up_sync(0xFFFFFFFFu, ib, o);
+        if (lane >= static_cast<uint32_t>(o)) {
+          ia += va;
+          ib += vb;
+        }
+      }
+      const uint32_t first_half = __shfl_sync(0xFFFFFFFFu, ia, 31);
+      if (lane < kModules) sh.mod_start[lane] = ia - a;
+      if (lane + 32 < kModules) sh.mod_start[lane + 32] = first_half + ib - a2;
+      const uint32_t total = first_half + __shfl_sync(0xFFFFFFFFu, ib, 31);
+      if (lane == 0) {
+        uint32_t fl = 0;
+        // the event's hit region is its raw word range: one hit per raw word
+        if (total > words || off / 4 + total > P.hit_capacity) fl |= kStatusHitOverflow;
+        if (sh.n_candidates > kMaxCandidatesEvent) fl |= kStatusCandidateOverflow;
+        if (fl) atomicOr(&sh.flags, fl);
+      }
+    }
+    __syncthreads();
+    const uint32_t base = static_cast<uint32_t>(off / 4);
+    const bool write = event_ok && !(sh.flags & kStatusHitOverflow);
+    // ---- emit pass: clusters into their module slice (slot order arbitrary) ----
+    if (write) {
+      for (uint32_t f = threadIdx.x; f < total_sp; f += blockDim.x) {
+        uint32_t b, cands;
+        ClusterPoint pts[2];
+        const uint32_t n = sp_clusters<true>(sh, ev, P, g, f, b, cands, pts);
+        if (!n) continue;
+        const uint32_t m = b >> 2;
+        const uint32_t slot = atomicAdd(&sh.mod_fill[m], n);
+        const bool odd = m & 1;
+        for (uint32_t c = 0; c < n; ++c) {
+          const uint32_t o = base + sh.mod_start[m] + slot + c;
+          P.hits.x[o] = pts[c].x;
+          P.hits.y[o] = pts[c].y;
+          P.hits.z[o] = pts[c].z;
+          P.hits.phi[o] = odd ? phi_odd_side(pts[c].x, pts[c].y) : phi_even_side(pts[c].x, pts[c].y);
+          P.hits.id[o] = pts[c].id;
+        }
+      }
+    }
+    __syncthreads();
+    // ---- per-module sort on (phi, LHCb id), in place ----
+    for (uint32_t m = warp; m < kModules; m += W) {
+      const uint32_t n = write ? sh.mod_count[m] : 0;
+      const uint32_t p0 = base + sh.mod_start[m];
+      if (n > kMaxHitsPerModule && lane == 0) atomicOr(&sh.flags, kStatusModuleOverflow);
+      if (n > 1 && n <= kSortCap) {
+        uint32_t size = 2;
+        while (size < n) size <<= 1;
+        for (uint32_t i = lane; i < size; i += 32) {
+          if (i < n) {
+            s_key[warp][i] = (static_cast<unsigned long long>(orderable(P.hits.phi[p0 + i])) << 32) | P.hits.id[p0 + i];
+            s_slot[warp][i] = static_cast<uint16_t>(i);
+          } else {
+            s_key[warp][i] = ~0ull;
+            s_slot[warp][i] = 0;
+          }
+        }
+        __syncwarp();
+        warp_bitonic_sort(s_key[warp], s_slot[warp], size);
+        // the keys are dead after the sort: their buffer stages the permutation
+        uint32_t* tmp = reinterpret_cast<uint32_t*>(s_key[warp]);
+        float* fields_f[4] = {P.hits.x, P.hits.y, P.hits.z, P.hits.phi};
+#pragma unroll 1
+        for (int a = 0; a < 5; ++a) {
+          uint32_t* arr = a < 4 ? reinterpret_cast<uint32_t*>(fields_f[a]) : P.hits.id;
+          for (uint32_t i = lane; i < n; i += 32) tmp[i] = arr[p0 + s_slot[warp][i]];
+          __syncwarp();
+          for (uint32_t i = lane; i < n; i += 32) arr[p0 + i] = tmp[i];
+          __syncwarp();
+        }
+      }
+      if (lane == 0) {
+        P.module_start[e * kModules + m] = p0;
+        P.module_num[e * kModules + m] = n;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      P.event_hit_base[e] = base;
+      P.event_hits[e] = write ? sh.mod_start[kModules - 1] + sh.mod_count[kModules - 1] : 0;
+      P.status[e] = sh.flags;
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace velo

@@ -67,11 +67,12 @@ constexpr uint32_t kMaxClusteringIterations = 12;
 constexpr uint8_t kCandidateKs[9] = {0, 0, 1, 4, 4, 5, 5, 5, 5};
 
 // Module z positions used by tracking (Constants.cu:27-31).
-constexpr float kModuleZ[kModules] = {
-  -287.5f, -275.f, -262.5f, -250.f, -237.5f, -225.f, -212.5f, -200.f, -137.5f, -125.f, -62.5f, -50.f, -37.5f,
-  -25.f,   -12.5f, 0.f,     12.5f,  25.f,    37.5f,  50.f,    62.5f,  75.f,    87.5f,  100.f,  112.5f, 125.f,
-  137.5f,  150.f,  162.5f,  175.f,  187.5f,  200.f,  212.5f,  225.f,  237.5f,  250.f,  262.5f, 275.f,  312.5f,
-  325.f,   387.5f, 400.f,   487.5f, 500.f,   587.5f, 600.f,   637.5f, 650.f,   687.5f, 700.f,  737.5f, 750.f};
+#define VELO_MODULE_Z_VALUES                                                                                      \
+  -287.5f, -275.f, -262.5f, -250.f, -237.5f, -225.f, -212.5f, -200.f, -137.5f, -125.f, -62.5f, -50.f, -37.5f,    \
+    -25.f, -12.5f, 0.f, 12.5f, 25.f, 37.5f, 50.f, 62.5f, 75.f, 87.5f, 100.f, 112.5f, 125.f, 137.5f, 150.f,        \
+    162.5f, 175.f, 187.5f, 200.f, 212.5f, 225.f, 237.5f, 250.f, 262.5f, 275.f, 312.5f, 325.f, 387.5f, 400.f,      \
+    487.5f, 500.f, 587.5f, 600.f, 637.5f, 650.f, 687.5f, 700.f, 737.5f, 750.f
+constexpr float kModuleZ[kModules] = {VELO_MODULE_Z_VALUES};
 
 // ---- raw event ----------------------------------------------------------------
 // u32 number_of_raw_banks, u32 raw_bank_offset[n+1] (byte offsets into the payload),

@@ -161,6 +161,8 @@ struct Geometry {
   const float* x_pitch;
   const float* ltg;
   float lo[kSensorColumns], hi[kSensorColumns];
+  double box[kSensors][4];  // global x/y bounding box of each sensor (xmin, xmax, ymin, ymax)
+  double z[kSensors];
   explicit Geometry(const void* blob)
   {
     GeometryView v = geometry_view(blob);
@@ -170,6 +172,21 @@ struct Geometry {
     for (uint32_t c = 0; c < kSensorColumns; ++c) {
       lo[c] = local_x[c] - 0.5f * x_pitch[c];
       hi[c] = local_x[c] + 0.5f * x_pitch[c];
+    }
+    const double w = hi[kSensorColumns - 1] + 0.01, h = kRows * kPixelSize + 0.01;
+    for (uint32_t s = 0; s < kSensors; ++s) {
+      const float* L = ltg + 16 * s;
+      double b[4] = {1e9, -1e9, 1e9, -1e9};
+      for (double u : {-0.01, w})
+        for (double v2 : {-0.01, h}) {
+          const double gx = L[0] * u + L[1] * v2 + L[9], gy = L[3] * u + L[4] * v2 + L[10];
+          b[0] = std::min(b[0], gx);
+          b[1] = std::max(b[1], gx);
+          b[2] = std::min(b[2], gy);
+          b[3] = std::max(b[3], gy);
+        }
+      for (int k = 0; k < 4; ++k) box[s][k] = b[k];
+      z[s] = L[11];
     }
   }
   // Column whose pixel contains lx (nearest centre when lx falls in an edge gap); -1 outside.
@@ -239,7 +256,8 @@ void generate_event(const VeloGenConfig& cfg, const Geometry& g, uint64_t index,
   const double noise_mean = cfg.noise_per_asic_per_nu * nu * (noisy ? cfg.noisy_factor : 1.0);
   const uint32_t n_pv = rng.poisson(nu * cfg.visible_fraction);
 
-  std::vector<std::vector<uint32_t>> pixels(kSensors);  // key = col<<8 | row
+  std::vector<uint32_t> pixels;  // key = sensor<<20 | col<<8 | row
+  pixels.reserve(4096);
   std::vector<McParticle> mcps;
 
   for (uint32_t v = 0; v < n_pv; ++v) {
@@ -266,10 +284,17 @@ void generate_event(const VeloGenConfig& cfg, const Geometry& g, uint64_t index,
       mcp.n_pv = n_pv;
       uint64_t modules_hit = 0;
 
+      uint8_t crossed[kSensors];
       for (uint32_t s = 0; s < kSensors; ++s) {
+        const double dzs = g.z[s] - z0;
+        const double gx = x0 + tx * dzs, gy = y0 + ty * dzs;
+        crossed[s] = (dzs * dir > 0) & (gx >= g.box[s][0]) & (gx <= g.box[s][1]) & (gy >= g.box[s][2]) &
+                     (gy <= g.box[s][3]);
+      }
+      for (uint32_t s = 0; s < kSensors; ++s) {
+        if (!crossed[s]) continue;
         const float* L = g.ltg + 16 * s;
         const double zs = L[11];
-        if ((zs - z0) * dir <= 0) continue;
         const double gx = x0 + tx * (zs - z0), gy = y0 + ty * (zs - z0);
         const double dx = gx - L[9], dy = gy - L[10];
         const double lx = L[0] * dx + L[3] * dy;
@@ -297,7 +322,7 @@ void generate_event(const VeloGenConfig& cfg, const Geometry& g, uint64_t index,
           if (cols[k] < 0 || cols[k] >= static_cast<int>(kSensorColumns) || rows[k] < 0 ||
               rows[k] >= static_cast<int>(kRows))
             continue;
-          pixels[s].push_back((static_cast<uint32_t>(cols[k]) << 8) | static_cast<uint32_t>(rows[k]));
+          pixels.push_back((s << 20) | (static_cast<uint32_t>(cols[k]) << 8) | static_cast<uint32_t>(rows[k]));
           sx += cols[k];
           sy += rows[k];
           ++m;
@@ -320,7 +345,7 @@ void generate_event(const VeloGenConfig& cfg, const Geometry& g, uint64_t index,
       for (uint32_t i = 0; i < k; ++i) {
         const uint32_t c = chip * kChipColumns + static_cast<uint32_t>(rng.next() % kChipColumns);
         const uint32_t r = static_cast<uint32_t>(rng.next() % kRows);
-        pixels[s].push_back((c << 8) | r);
+        pixels.push_back((s << 20) | (c << 8) | r);
       }
     }
   for (auto& m : mcps) m.n_pv = n_pv;
@@ -331,21 +356,21 @@ void generate_event(const VeloGenConfig& cfg, const Geometry& g, uint64_t index,
   const size_t offs_at = ev.raw.size();
   ev.raw.resize(offs_at + kSensors + 1, 0);
   const size_t payload_at = ev.raw.size();
-  std::vector<std::pair<uint32_t, uint32_t>> sps;  // (addr, mask)
+  std::sort(pixels.begin(), pixels.end());
+  pixels.erase(std::unique(pixels.begin(), pixels.end()), pixels.end());
+  std::vector<std::pair<uint32_t, uint32_t>> sps, merged;  // (addr, mask)
+  std::vector<uint64_t> occupancy(384, 0);
+  size_t p = 0;
   for (uint32_t s = 0; s < kSensors; ++s) {
-    auto& px = pixels[s];
-    std::sort(px.begin(), px.end());
-    px.erase(std::unique(px.begin(), px.end()), px.end());
     sps.clear();
-    for (uint32_t key : px) {
-      const uint32_t c = key >> 8, r = key & 0xFF;
+    for (; p < pixels.size() && (pixels[p] >> 20) == s; ++p) {
+      const uint32_t c = (pixels[p] >> 8) & 0xFFF, r = pixels[p] & 0xFF;
       const uint32_t addr = ((c >> 1) << 6) | (r >> 2);
       const uint32_t bit = 1u << (((c & 1u) << 2) | (r & 3u));
-      if (!sps.empty() && sps.back().first == addr) sps.back().second |= bit;
-      else sps.emplace_back(addr, bit);
+      sps.emplace_back(addr, bit);
     }
     std::sort(sps.begin(), sps.end());
-    std::vector<std::pair<uint32_t, uint32_t>> merged;
+    merged.clear();
     for (auto& e : sps) {
       if (!merged.empty() && merged.back().first == e.first) merged.back().second |= e.second;
       else merged.push_back(e);
@@ -353,23 +378,18 @@ void generate_event(const VeloGenConfig& cfg, const Geometry& g, uint64_t index,
     ev.raw[offs_at + s] = static_cast<uint32_t>((ev.raw.size() - payload_at) * 4);
     ev.raw.push_back(s);
     ev.raw.push_back(static_cast<uint32_t>(merged.size()));
-    auto has = [&](int32_t c, int32_t r) {
-      if (c < 0 || r < 0 || c >= 384 || r >= 64) return false;
-      const uint32_t a = (static_cast<uint32_t>(c) << 6) | static_cast<uint32_t>(r);
-      auto it = std::lower_bound(merged.begin(), merged.end(), std::make_pair(a, 0u));
-      return it != merged.end() && it->first == a;
-    };
+    // occupancy of SP columns: one 64-bit row mask per SP column (384 columns)
+    for (auto& e : merged) occupancy[e.first >> 6] |= 1ull << (e.first & 0x3F);
     for (auto& e : merged) {
       const int32_t c = e.first >> 6, r = e.first & 0x3F;
-      bool iso = true;
-      for (int dc = -1; dc <= 1 && iso; ++dc)
-        for (int dr = -1; dr <= 1; ++dr)
-          if ((dc || dr) && has(c + dc, r + dr)) {
-            iso = false;
-            break;
-          }
-      ev.raw.push_back(make_sp_word(c, r, e.second, iso));
+      const uint64_t rows3 = (r > 0 ? 7ull << (r - 1) : 3ull) & ~0ull;  // rows r-1..r+1
+      const uint64_t self = 1ull << r;
+      uint64_t near = (occupancy[c] & rows3 & ~self);
+      if (c > 0) near |= occupancy[c - 1] & rows3;
+      if (c < 383) near |= occupancy[c + 1] & rows3;
+      ev.raw.push_back(make_sp_word(c, r, e.second, near == 0));
     }
+    for (auto& e : merged) occupancy[e.first >> 6] = 0;
   }
   ev.raw[offs_at + kSensors] = static_cast<uint32_t>((ev.raw.size() - payload_at) * 4);
   ev.mc.clear();

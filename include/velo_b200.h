@@ -194,6 +194,12 @@ int velo_set_timing(VeloCtx* ctx, int enabled);
 
 int velo_destroy(VeloCtx* ctx);
 
+/* Blocking copy of device memory of the context's device into host memory (for callers
+ * without their own CUDA runtime, e.g. FFI bindings reading the outputs). */
+int velo_download(VeloCtx* ctx, void* dst_host, const void* src_device, size_t bytes);
+/* Asynchronous variant on `stream` (dst_host should be pinned). */
+int velo_download_async(VeloCtx* ctx, void* dst_host, const void* src_device, size_t bytes, void* stream);
+
 /* Kernel launch count of the last run (all kernels of this library). */
 int velo_last_launch_count(VeloCtx* ctx, uint32_t* n);
 

@@ -122,3 +122,134 @@ def sp_luts():
     fy = np.zeros(512, np.float32)
     L.oracle_sp_luts(pat.ctypes.data, fx.ctypes.data, fy.ctypes.data)
     return pat, fx, fy
+
+
+# ---------------------------------------------------------------------------
+# The reference's own CUDA kernels (oracle/_ref/libvelo_ref_gpu.so)
+# ---------------------------------------------------------------------------
+class RefOutputs(C.Structure):
+    _fields_ = [("n_events", C.c_uint32), ("total_estimated", C.c_uint32), ("total_tracks", C.c_uint32),
+                ("total_track_hits", C.c_uint32), ("module_start", C.POINTER(C.c_uint32)),
+                ("module_num", C.POINTER(C.c_uint32)), ("container", C.POINTER(C.c_uint32)),
+                ("candidate_num", C.POINTER(C.c_uint32)), ("weak_num", C.POINTER(C.c_uint32)),
+                ("atomics", C.POINTER(C.c_uint32)), ("track_hit_number", C.POINTER(C.c_uint32)),
+                ("track_hits", C.POINTER(C.c_uint8)), ("states", C.POINTER(C.c_uint8)),
+                ("kalman", C.POINTER(C.c_uint8))]
+
+
+_ref_gpu = None
+
+
+def ref_gpu_lib():
+    global _ref_gpu
+    if _ref_gpu is None:
+        if not os.path.exists(REF_GPU_LIB):
+            raise RuntimeError(f"{REF_GPU_LIB} missing: run oracle/build.py where the reference tree exists")
+        L = C.CDLL(REF_GPU_LIB)
+        P = C.c_void_p
+        L.ref_velo_run.argtypes = [P, P, C.c_uint32, P, C.c_int, C.POINTER(C.c_float), C.POINTER(RefOutputs)]
+        L.ref_velo_run.restype = C.c_int
+        L.ref_free.argtypes = [C.POINTER(RefOutputs)]
+        L.ref_state_size.restype = C.c_int
+        _ref_gpu = L
+    return _ref_gpu
+
+
+def _np(ptr, dtype, count):
+    if count == 0:
+        return np.zeros(0, dtype)
+    return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(np.ctypeslib.as_ctypes_type(dtype))), shape=(count,)).copy()
+
+
+def ref_gpu_run(batch, geometry, reps=1):
+    """Runs the reference's VELO kernels on the GPU. Returns (dict of numpy arrays, ms per rep).
+    Only events that fit the reference's fixed buffers may be passed (see ref_harness.cu)."""
+    L = ref_gpu_lib()
+    off32 = batch.offsets.astype(np.uint32)
+    out = RefOutputs()
+    ms = C.c_float()
+    rc = L.ref_velo_run(batch.raw.ctypes.data, off32.ctypes.data, batch.n_events, geometry.ctypes.data, reps,
+                        C.byref(ms), C.byref(out))
+    if rc != 0:
+        raise RuntimeError(f"ref_velo_run failed: {rc}")
+    try:
+        N, S, T, H = out.n_events, out.total_estimated, out.total_tracks, out.total_track_hits
+        ss = L.ref_state_size()
+        cont = _np(out.container, np.uint32, 6 * S)
+        res = dict(module_start=_np(out.module_start, np.uint32, N * NM + 1),
+                   module_num=_np(out.module_num, np.uint32, N * NM),
+                   y=cont[0:S].view(np.float32), z=cont[S:2 * S].view(np.float32), id=cont[2 * S:3 * S],
+                   phi=cont[4 * S:5 * S].view(np.float32), x=cont[5 * S:6 * S].view(np.float32),
+                   candidate_num=_np(out.candidate_num, np.uint32, N), weak_num=_np(out.weak_num, np.uint32, N),
+                   atomics=_np(out.atomics, np.uint32, 2 * N + 1),
+                   track_hit_number=_np(out.track_hit_number, np.uint32, T + 1),
+                   track_hits=_np(out.track_hits, np.uint8, 16 * H), states=_np(out.states, np.uint8, ss * T),
+                   kalman=_np(out.kalman, np.uint8, ss * T))
+        hv = res["track_hits"].view(np.float32).reshape(4, H) if H else np.zeros((4, 0), np.float32)
+        res["hit_x"], res["hit_y"], res["hit_z"], res["hit_id"] = hv[0], hv[1], hv[2], hv[3].view(np.uint32)
+        res["n_tracks"] = res["atomics"][:N]
+        res["track_offsets"] = res["atomics"][N:2 * N + 1]
+        res["T"], res["H"] = T, H
+        return res, ms.value
+    finally:
+        L.ref_free(C.byref(out))
+
+
+def ref_event_clusters(res, e):
+    out = []
+    for m in range(NM):
+        s, n = int(res["module_start"][e * NM + m]), int(res["module_num"][e * NM + m])
+        out.append({k: res[k][s:s + n] for k in ("x", "y", "z", "phi", "id")})
+    return out
+
+
+def ref_decode_states(res, key):
+    """SoA states of the reference (layout VeloConsolidated.cuh:68-144) -> dict of arrays."""
+    T = res["T"]
+    blob = res[key].tobytes()
+    f = np.frombuffer(blob, dtype=np.float32, count=12 * T).reshape(12, T) if T else np.zeros((12, 0), np.float32)
+    out = {k: f[i].copy() for i, k in enumerate(STATE_FIELDS[:12])}
+    out["backward"] = np.frombuffer(blob, dtype=np.uint8, count=T, offset=48 * T).astype(bool) if T else np.zeros(0, bool)
+    return out
+
+
+# ---------------------------------------------------------------------------
+# The reference's x86 clustering (oracle/_ref/libvelo_ref_x86.so)
+# ---------------------------------------------------------------------------
+_ref_x86 = None
+
+
+def ref_x86_clustering(batch, geometry, algo=1, threads=0):
+    """algo 0: clustering() (classic), 1: cuda_clustering_cpu_optimized(). Returns (counts, ids, id_offsets)."""
+    global _ref_x86
+    if _ref_x86 is None:
+        if not os.path.exists(REF_X86_LIB):
+            raise RuntimeError(f"{REF_X86_LIB} missing")
+        _ref_x86 = C.CDLL(REF_X86_LIB)
+        P = C.c_void_p
+        _ref_x86.ref_x86_clustering.argtypes = [P, P, C.c_uint32, P, C.c_int, C.c_int, P, P, C.c_uint64, P]
+        _ref_x86.ref_x86_clustering.restype = C.c_int
+    N = batch.n_events
+    off32 = batch.offsets.astype(np.uint32)
+    counts = np.zeros(N, np.uint32)
+    cap = int(batch.raw.size)
+    ids = np.zeros(cap, np.uint32)
+    io = np.zeros(N + 1, np.uint64)
+    rc = _ref_x86.ref_x86_clustering(batch.raw.ctypes.data, off32.ctypes.data, N, geometry.ctypes.data, algo,
+                                     threads, counts.ctypes.data, ids.ctypes.data, cap, io.ctypes.data)
+    if rc != 0:
+        raise RuntimeError(f"ref_x86_clustering failed: {rc}")
+    return counts, ids, io
+
+
+def ref_x86_sp_patterns():
+    ref_x86_clustering  # noqa: B018 (library handle is created below)
+    L = C.CDLL(REF_X86_LIB)
+    P = C.c_void_p
+    L.ref_x86_sp_patterns.argtypes = [P, P, P, P]
+    pat = np.zeros(256, np.uint8)
+    siz = np.zeros(256, np.uint8)
+    fx = np.zeros(512, np.float32)
+    fy = np.zeros(512, np.float32)
+    L.ref_x86_sp_patterns(pat.ctypes.data, siz.ctypes.data, fx.ctypes.data, fy.ctypes.data)
+    return pat, siz, fx, fy

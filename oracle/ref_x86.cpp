@@ -13,6 +13,18 @@
 
 extern "C" {
 
+// The reference's SuperPixel tables (x86/velo/clustering/src/ClusteringCommon.cpp:3-101).
+void ref_x86_sp_patterns(uint8_t* patterns, uint8_t* sizes, float* fx, float* fy)
+{
+  std::vector<unsigned char> p(256, 0), s(256, 0);
+  std::vector<float> x(512, 0), y(512, 0);
+  cache_sp_patterns(p, s, x, y);
+  std::memcpy(patterns, p.data(), 256);
+  std::memcpy(sizes, s.data(), 256);
+  std::memcpy(fx, x.data(), 512 * sizeof(float));
+  std::memcpy(fy, y.data(), 512 * sizeof(float));
+}
+
 // algo: 0 = clustering (classic flood fill), 1 = cuda_clustering_cpu_optimized.
 // Splits the events into contiguous slices, one reference call per slice, over n_threads
 // host threads. counts[N] receives the clusters per event; ids (optional, capacity

@@ -1,0 +1,217 @@
+"""Parity of the CUDA chain (through the C ABI) with the reference.
+
+Bit-exact bar (integer work and the float values the reference computes):
+  * clusters: count per module, LHCb ids and per-module order, x/y/z/phi bit for bit;
+    within a module the reference's order for exactly equal phi follows its atomics, so
+    only permutations of equal-phi entries are tolerated;
+  * tracks: per-event hit-id lists identical after a canonical sort;
+  * beamline (LSQ) and Kalman states: all 12 floats bit for bit (bound of the north star:
+    1e-5 relative), `backward` of the beamline state equal.
+Events the reference leaves undefined (buffer spills, reads outside a module, exact
+scatter ties resolved by atomics) are flagged by both sides and excluded.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+import parity_utils as pu
+from conftest import golden_batch, golden_event_clusters, golden_event_tracks, load_golden
+from cuda_hlt_b200 import chain, events
+
+pytestmark = pytest.mark.gpu
+
+
+def run_chain(b, **kw):
+    vc = chain.VeloChain(max_events=max(1, b.n_events), max_raw_bytes=int(b.raw.size) + 4096, **kw)
+    vc.run_host(b)
+    vc.sync()
+    res = vc.results()
+    vc.close()
+    return res
+
+
+def assert_clusters_equal(mine_mods, ref_mods, ctx):
+    for m, (a, r) in enumerate(zip(mine_mods, ref_mods)):
+        assert len(a["id"]) == len(r["id"]), (ctx, m)
+        same_phi = np.array_equal(pu.bits(a["phi"]), pu.bits(r["phi"]))
+        assert same_phi, (ctx, m, "phi")
+        if np.array_equal(a["id"], r["id"]):
+            for k in ("x", "y", "z"):
+                assert np.array_equal(pu.bits(a[k]), pu.bits(r[k])), (ctx, m, k)
+        else:
+            # only permutations inside runs of equal phi
+            phis = pu.bits(a["phi"])
+            for v in np.unique(phis):
+                sel = phis == v
+                key_a = sorted(zip(a["id"][sel], pu.bits(a["x"][sel]), pu.bits(a["y"][sel]), pu.bits(a["z"][sel])))
+                key_r = sorted(zip(r["id"][sel], pu.bits(r["x"][sel]), pu.bits(r["y"][sel]), pu.bits(r["z"][sel])))
+                assert key_a == key_r, (ctx, m)
+
+
+def assert_states_equal(mine, e, mt, g_states, g_tracks, t0g, ctx):
+    gi = pu.track_index(g_tracks)
+    t0m = int(mine["track_offsets"][e])
+    for i, t in enumerate(mt):
+        j = gi[t]
+        for which in ("states", "kalman"):
+            for key in pu.STATE_KEYS:
+                got = np.float32(mine[which][key][t0m + i])
+                ref = np.float32(g_states[f"{which}_{key}"][t0g + j])
+                assert got.view(np.uint32) == ref.view(np.uint32), (ctx, which, key, got, ref)
+        assert bool(mine["states"]["backward"][t0m + i]) == bool(g_states["states_backward"][t0g + j])
+
+
+@pytest.mark.parametrize("which", ["minbias", "plain", "batched"])
+def test_bit_exact_against_reference_golden(which):
+    g = load_golden(which)
+    b = golden_batch(which)
+    res = run_chain(b)
+    N = b.n_events
+    compared = 0
+    for e in range(N):
+        if res["status"][e] & chain.REFERENCE_UNDEFINED:
+            continue
+        assert_clusters_equal(chain.event_clusters(res, e), golden_event_clusters(g, e), (which, e))
+        mt, gt = chain.event_tracks(res, e), golden_event_tracks(g, e)
+        assert pu.canonical_tracks(mt) == pu.canonical_tracks(gt), (which, e)
+        assert_states_equal(res, e, mt, g, gt, int(g["atomics"][N + e]), (which, e))
+        compared += 1
+    assert compared >= N - 2
+
+
+@pytest.mark.skipif(not os.path.exists(oracle.REF_GPU_LIB), reason="reference GPU build missing")
+@pytest.mark.parametrize("config,n", [("plain_1k", 300), ("batched_500k", 300), ("high_occupancy_200k", 60)])
+def test_bit_exact_against_reference_kernels_live(geometry, config, n):
+    """The reference's own kernels run on the same events in the same process."""
+    b = events.generate_config(config, n_events=n, first_event=1000)
+    # Events whose reference run spills past its per-event buffers would also corrupt the
+    # following events of the reference's batch: they are left out of the batch.
+    orc = oracle.run(b, geometry)
+    keep = [e for e in range(n) if not (orc.flags[e] & oracle.UNDEFINED_IN_REFERENCE)
+            and orc.module_num[e * 52:(e + 1) * 52].max() < 500]
+    sub = events.EventBatch(np.concatenate([b.event(e) for e in keep]),
+                            np.concatenate([[0], np.cumsum([b.event(e).size for e in keep])]).astype(np.uint64))
+    ref, _ = oracle.ref_gpu_run(sub, geometry)
+    res = run_chain(sub)
+    N = sub.n_events
+    rs = {k: oracle.ref_decode_states(ref, k) for k in ("states", "kalman")}
+    flat = {f"{w}_{k}": v for w in rs for k, v in rs[w].items()}
+    compared = 0
+    for e in range(N):
+        if res["status"][e] & chain.REFERENCE_UNDEFINED:
+            continue
+        assert_clusters_equal(chain.event_clusters(res, e), oracle.ref_event_clusters(ref, e), (config, e))
+        mt, rt = chain.event_tracks(res, e), chain.event_tracks(ref, e)
+        assert pu.canonical_tracks(mt) == pu.canonical_tracks(rt), (config, e)
+        assert_states_equal(res, e, mt, flat, rt, int(ref["track_offsets"][e]), (config, e))
+        compared += 1
+    assert compared >= 0.95 * N
+
+
+def test_against_cpu_oracle(geometry):
+    b = events.generate_config("plain_1k", n_events=200, first_event=500)
+    res = run_chain(b)
+    r = oracle.run(b, geometry)
+    diff = total = 0
+    for e in range(b.n_events):
+        oc = r.event_clusters(e)
+        got = np.concatenate([m["id"] for m in chain.event_clusters(res, e)])
+        assert np.array_equal(np.sort(got), np.sort(oc["id"])), e
+        a, bb = pu.compare_event_tracks(chain.event_tracks(res, e), r.event_tracks(e))
+        diff += a + bb
+        total += len(r.event_tracks(e))
+    assert diff <= 0.005 * total, (diff, total)
+
+
+def test_deterministic_and_graph_equal():
+    b = events.generate_config("batched_500k", n_events=257, first_event=77)
+    r1 = run_chain(b)
+    r2 = run_chain(b)
+    r3 = run_chain(b, use_graphs=True)
+    for k in ("atomics", "track_hit_number", "hit_id", "hit_x", "status", "module_num", "cluster_id", "cluster_phi"):
+        assert np.array_equal(r1[k], r2[k]), k
+        assert np.array_equal(r1[k], r3[k]), k
+    for k in pu.STATE_KEYS:
+        assert np.array_equal(pu.bits(r1["kalman"][k]), pu.bits(r3["kalman"][k])), k
+
+
+def test_host_and_device_input_paths_agree():
+    import torch
+    b = events.generate_config("plain_1k", n_events=50)
+    ref = run_chain(b)
+    raw = torch.from_numpy(b.raw).cuda()
+    off = torch.from_numpy(b.offsets.view(np.int64)).cuda()
+    vc = chain.VeloChain(max_events=50, max_raw_bytes=int(b.raw.size))
+    vc.run_device(raw.data_ptr(), off.data_ptr(), 50, torch.cuda.current_stream().cuda_stream)
+    vc.sync()
+    res = vc.results()
+    vc.close()
+    for k in ("atomics", "track_hit_number", "hit_id", "module_num"):
+        assert np.array_equal(ref[k], res[k]), k
+
+
+def _empty_event():
+    nb = 208
+    payload, offs = [], [0]
+    for k in range(nb):
+        payload += [k, 0]
+        offs.append(4 * len(payload))
+    return np.array([nb] + offs + payload, np.uint32).view(np.uint8)
+
+
+def test_edge_cases_empty_corrupt_and_ragged(geometry):
+    good = events.generate_config("plain_1k", n_events=5)
+    empty = _empty_event()
+    corrupt = good.event(2).copy().view(np.uint32)
+    corrupt[3] = 0xFFFFFF00  # bank offset far outside the event
+    truncated = good.event(3)[:500]
+    parts = [good.event(0), empty, corrupt.view(np.uint8), good.event(1), truncated, good.event(4)]
+    raw = np.concatenate(parts)
+    offs = np.concatenate([[0], np.cumsum([p.size for p in parts])]).astype(np.uint64)
+    res = run_chain(events.EventBatch(raw, offs))
+    st = res["status"]
+    assert st[0] == 0 and st[1] == 0 and st[3] == 0 and st[5] == 0
+    assert st[2] & chain.STATUS["bad_raw"] and st[4] & chain.STATUS["bad_raw"]
+    assert res["n_tracks"][1] == res["n_tracks"][2] == res["n_tracks"][4] == 0
+    clean = run_chain(good)
+    for mine_e, clean_e in ((0, 0), (3, 1), (5, 4)):
+        assert pu.canonical_tracks(chain.event_tracks(res, mine_e)) == \
+            pu.canonical_tracks(chain.event_tracks(clean, clean_e))
+    # an empty batch
+    vc = chain.VeloChain(max_events=4, max_raw_bytes=1 << 16)
+    vc.run_host(events.EventBatch(np.zeros(0, np.uint8), np.zeros(1, np.uint64)))
+    t, h, c = vc.sync()
+    assert (t, h, c) == (0, 0, 0)
+    vc.close()
+
+
+def test_capacity_errors():
+    b = events.generate_config("plain_1k", n_events=8)
+    vc = chain.VeloChain(max_events=4, max_raw_bytes=int(b.raw.size))
+    with pytest.raises(chain.VeloError):
+        vc.run_host(b)
+    vc.close()
+
+
+def test_full_size_batch_properties():
+    """16,384 events of the nu ~ U(2,15) workload: consistent offsets and layouts."""
+    b = events.generate_config("batched_500k", n_events=16384, first_event=100000, with_mc=False)
+    res = run_chain(b)
+    N = b.n_events
+    at = res["atomics"]
+    assert np.array_equal(np.cumsum(np.concatenate([[0], at[:N]])), at[N:2 * N + 1])
+    thn = res["track_hit_number"]
+    n_hits = np.diff(thn)
+    assert np.all(n_hits >= 3) and np.all(n_hits <= 26)
+    # consolidated hit ids are clusters of the event and hits of a track are in distinct modules
+    for e in range(0, N, 997):
+        ids = set(np.concatenate([m["id"] for m in chain.event_clusters(res, e)]).tolist())
+        for t in chain.event_tracks(res, e):
+            assert set(t) <= ids
+            mods = [(i >> 20) & 0x3F for i in t]  # sensor >> 2
+            assert len(set(mods)) == len(mods)
+    for k in pu.STATE_KEYS:
+        assert np.all(np.isfinite(res["states"][k]))
+    assert (res["status"] & chain.STATUS["bad_raw"]).sum() == 0
