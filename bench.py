@@ -172,6 +172,9 @@ def run_ours(args, rank, world, local_rank):
 
     vc = chain.VeloChain(max_events=BUCKET, max_raw_bytes=max_batch_bytes + 4096, device=local_rank,
                          use_graphs=True)
+    # search mapping per hit-count bucket, tuned on the first batch (outside the timed region)
+    from cuda_hlt_b200 import autotune
+    threshold, tune_ms = autotune.tune_block_threshold(vc, *batch_ptrs[0], stream)
     vc.set_timing(True)
 
     # census: per-batch totals for the algorithmic-byte accounting
@@ -234,7 +237,7 @@ def run_ours(args, rank, world, local_rank):
         traffic = tr["bytes_per_event"][dominant] * n_events / n_batches
 
     # ---- end to end through velo_run_host with host buffers ----
-    e2e = run_e2e(args, chunks, plan, local_rank, torch, world, dist)
+    e2e = run_e2e(args, chunks, plan, local_rank, torch, world, dist, threshold)
 
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -243,6 +246,8 @@ def run_ours(args, rank, world, local_rank):
         "config": {"workload": f"{WORKLOAD}: {n_events} events per GPU, pileup nu ~ U(2,15), seed 0, "
                                f"events rank*{n_events}...", "events_per_gpu": n_events, "batch_events": BUCKET,
                    "batches_per_step": n_batches, "mode": "plain", "graphs": True,
+                   "search_mapping": {"block_above_clusters": threshold,
+                                      "search_ms_per_threshold": {str(k): v for k, v in tune_ms.items()}},
                    "l2": f"inputs larger than L2 ({raw_bytes / 1e9:.2f} GB raw banks per step)",
                    "parallelism": f"event shards x{world}"},
         "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "peak_source": peak_kind,
@@ -260,7 +265,7 @@ def run_ours(args, rank, world, local_rank):
     return result, chunks
 
 
-def run_e2e(args, chunks, plan, local_rank, torch, world, dist):
+def run_e2e(args, chunks, plan, local_rank, torch, world, dist, threshold):
     """velo_run_host from pinned memory, two contexts alternating on two streams so that
     the copies of one batch overlap the kernels of the other; outputs read back to pinned
     host buffers every batch."""
@@ -275,6 +280,8 @@ def run_e2e(args, chunks, plan, local_rank, torch, world, dist):
     max_batch_bytes = max(int(chunks[ci].offsets[b] - chunks[ci].offsets[a]) for ci, a, b in plan)
     ctxs = [chain.VeloChain(max_events=BUCKET, max_raw_bytes=max_batch_bytes + 4096, device=local_rank)
             for _ in range(2)]
+    for vc in ctxs:
+        vc.set_block_threshold(threshold)
     streams = [torch.cuda.Stream(device=local_rank) for _ in range(2)]
     # pinned result buffers per context: atomics, hit numbers, hits SoA, Kalman states
     cap_t = 400 * BUCKET
@@ -380,7 +387,7 @@ def reference_gpu(batch):
     # events that overrun the reference's fixed per-event buffers would spill into their
     # neighbours; they are left out so that the reference run stays well defined
     keep = [e for e in range(batch.n_events) if r.module_num[e * 52:(e + 1) * 52].max() < 500
-            and not (r.flags[e] & oracle.UNDEFINED_IN_REFERENCE & ~oracle.F_SEED_TIE)]
+            and not (int(r.flags[e]) & (oracle.UNDEFINED_IN_REFERENCE & ~oracle.F_SEED_TIE))]
     sub = events.EventBatch(np.concatenate([batch.event(e) for e in keep]),
                             np.concatenate([[0], np.cumsum([batch.event(e).size for e in keep])]).astype(np.uint64))
     _, ms = oracle.ref_gpu_run(sub, geo, reps=4)

@@ -74,10 +74,7 @@ class VeloOutputs(C.Structure):
         ("status", C.c_void_p),
         ("module_hit_start", C.c_void_p),
         ("module_hit_num", C.c_void_p),
-        ("hit_x", C.c_void_p),
-        ("hit_y", C.c_void_p),
-        ("hit_z", C.c_void_p),
-        ("hit_phi", C.c_void_p),
+        ("hit_xyzp", C.c_void_p),
         ("hit_id", C.c_void_p),
         ("hit_capacity", C.c_uint64),
     ]
@@ -106,6 +103,7 @@ GPU_SYMBOLS = [
     "velo_destroy",
     "velo_download",
     "velo_download_async",
+    "velo_set_block_threshold",
     "velo_last_launch_count",
     "velo_version",
 ]
@@ -171,6 +169,8 @@ def gpu_lib():
         lib.velo_download.restype = C.c_int
         lib.velo_download_async.argtypes = [P, P, P, C.c_size_t, P]
         lib.velo_download_async.restype = C.c_int
+        lib.velo_set_block_threshold.argtypes = [P, C.c_uint32]
+        lib.velo_set_block_threshold.restype = C.c_int
         lib.velo_last_launch_count.argtypes = [P, C.POINTER(C.c_uint32)]
         lib.velo_last_launch_count.restype = C.c_int
         lib.velo_version.argtypes = []

@@ -124,6 +124,10 @@ class VeloChain:
         out["runs"] = int(ms[4])
         return out
 
+    def set_block_threshold(self, clusters):
+        """Events above `clusters` clusters use the block-per-event search, others the warp one."""
+        _check(self.lib.velo_set_block_threshold(self.ctx, int(clusters)), "velo_set_block_threshold")
+
     def launch_count(self):
         n = C.c_uint32()
         _check(self.lib.velo_last_launch_count(self.ctx, C.byref(n)), "velo_last_launch_count")
@@ -157,9 +161,10 @@ class VeloChain:
             res["module_start"] = self._down(o.module_hit_start, np.uint32, N * N_MODULES)
             res["module_num"] = self._down(o.module_hit_num, np.uint32, N * N_MODULES)
             span = int((res["module_start"] + res["module_num"]).max()) if N else 0
-            for k, p, dt in (("x", o.hit_x, np.float32), ("y", o.hit_y, np.float32), ("z", o.hit_z, np.float32),
-                             ("phi", o.hit_phi, np.float32), ("id", o.hit_id, np.uint32)):
-                res["cluster_" + k] = self._down(p, dt, span)
+            xyzp = self._down(o.hit_xyzp, np.float32, 4 * span).reshape(span, 4)
+            for i, k in enumerate(("x", "y", "z", "phi")):
+                res["cluster_" + k] = np.ascontiguousarray(xyzp[:, i])
+            res["cluster_id"] = self._down(o.hit_id, np.uint32, span)
         return res
 
 

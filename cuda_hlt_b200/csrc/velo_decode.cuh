@@ -1,14 +1,20 @@
 // Kernel 1 of the chain: SuperPixel decode, masked clustering, phi and per-module sort.
 //
-// One block per event (persistent; events are pulled from a device queue). Work is flat
-// over the event's SP words: each thread takes SPs, finds the neighbouring SPs it needs by
-// binary search in the bank (banks are address-sorted in LHCb raw data; unsorted banks
-// fall back to the reference's linear scan, with the same result), clusters, and appends
-// the clusters to its module's slice of the event's hit region. The module slices are
-// then sorted in place on (phi, LHCb id) by one warp each (bitonic network in shared
-// memory). The result equals the reference's estimate -> prefix sum -> masked clustering
-// -> calculate_phi_and_sort sequence, whose slot order within a module is atomic-order
-// dependent only for exactly equal phi.
+// One block per event (persistent; events are pulled from a device queue), one pass over
+// the event's SP words:
+//   * isolated SPs give their one or two clusters from the pattern table at once;
+//   * a non-isolated SP finds its neighbours by binary search in its bank (banks are
+//     address-sorted in LHCb raw data; unsorted banks fall back to the reference's linear
+//     scan, with the same result) and pushes its candidate pixels to a shared list, which
+//     the block then flood-fills with every thread busy;
+//   * clusters go to their module's slice of a staging area sized by the module's SP count
+//     (at most two clusters per SP), one shared atomic per cluster;
+//   * one warp per module sorts the slice on the key (phi, LHCb id) - in registers with
+//     warp shuffles up to 128 clusters, in shared memory up to 512 - and writes it to the
+//     compact phi-sorted layout.
+// The result equals the reference's estimate -> prefix sum -> masked clustering ->
+// calculate_phi_and_sort sequence, whose order within a module depends on the order of its
+// atomics only for exactly equal phi.
 #pragma once
 #include "velo_kernels.cuh"
 
@@ -151,105 +157,120 @@ __device__ __forceinline__ bool flood_window(uint32_t px0, uint32_t px1, uint32_
   return true;
 }
 
+constexpr uint32_t kCandCap = 4096;    // candidate pixels listed per event (more: flooded inline)
+constexpr uint32_t kRegSortMax = 128;  // modules up to this size are sorted in registers
+
 struct DecodeShared {
   uint32_t bank_start[kSensors];  // word index (from the event start) of the first SP word
   uint32_t bank_count[kSensors];
   uint32_t bank_sensor[kSensors];
   uint32_t sp_prefix[kSensors + 1];  // exclusive scan of bank_count
   uint32_t unsorted[(kSensors + 31) / 32];
-  uint32_t mod_count[kModules];
-  uint32_t mod_start[kModules];
-  uint32_t mod_fill[kModules];
+  uint32_t mod_count[kModules];  // clusters per module
+  uint32_t mod_start[kModules];  // exclusive scan of mod_count: compact layout
   uint32_t event;
   uint32_t flags;
   uint32_t n_candidates;
+  uint32_t n_list;
 };
 
-// Clusters of SP number f of the event (flat over banks). Returns the cluster count; with
-// emit, the clusters are placed into pts.
-template<bool emit>
-__device__ __forceinline__ uint32_t sp_clusters(const DecodeShared& sh, const uint32_t* ev, const ChainPointers& P,
-                                                const GeometryView& g, uint32_t f, uint32_t& bank_out,
-                                                uint32_t& cands, ClusterPoint* pts)
+__device__ __forceinline__ uint32_t bank_of(const DecodeShared& sh, uint32_t f)
 {
-  // bank of flat index f: last b with sp_prefix[b] <= f
-  uint32_t lo = 0, hi = kSensors;
+  uint32_t lo = 0, hi = kSensors;  // last b with sp_prefix[b] <= f
   while (hi - lo > 1) {
     const uint32_t mid = (lo + hi) >> 1;
     if (sh.sp_prefix[mid] <= f) lo = mid; else hi = mid;
   }
-  const uint32_t b = lo;
-  bank_out = b;
-  const uint32_t s = f - sh.sp_prefix[b];
-  const uint32_t* bank = ev + sh.bank_start[b];
-  const uint32_t count = sh.bank_count[b];
-  const uint32_t sensor = sh.bank_sensor[b];
-  const bool sorted = !((sh.unsorted[b >> 5] >> (b & 31)) & 1u);
-  const uint32_t word = __ldg(bank + s);
-  const uint32_t sp = sp_mask(word);
-  const int32_t sp_r = sp_row(word), sp_c = sp_col(word);
-  uint32_t n = 0;
-  cands = 0;
-  if (sp_isolated(word)) {
-    // isolated SP: pattern table (MaskedVeloClustering.cu:105-167)
-    const uint32_t idx = __ldg(P.k.sp_patterns + sp);
-    n = 1 + ((idx >> 3) & 1u);
-    if (emit) {
-      const uint32_t chip = sp_c / (kChipColumns / 2);
-#pragma unroll
-      for (int c = 0; c < 2; ++c) {
-        if (c == 1 && !(idx & 8)) break;
-        const uint32_t row = c ? (idx >> 4) & 3u : idx & 0x03u;
-        const uint32_t col = c ? (idx >> 6) & 1u : (idx >> 2) & 1u;
-        const uint32_t cx = sp_c * 2 + col;
-        const uint32_t cy = sp_r * 4 + row;
-        const float fx = __ldg(P.k.sp_fx + sp * 2 + c);
-        const float fy = __ldg(P.k.sp_fy + sp * 2 + c);
-        pts[c] = place_cluster(g, sensor, cx, cy, fx, fy, chip);
-      }
-    }
-    return n;
-  }
-  const SpWindow w = gather_window(bank, count, sorted, sp_r, sp_c);
-  const uint32_t code = window_candidate_code(sp, w);
-  if (!code) return 0;
-  // The reference packs the SP index into a u8 when it decodes candidates
-  // (MaskedVeloClustering.cu:179), so above 255 SPs the flood runs on SP s & 0xFF.
-  const uint32_t s2 = s & 0xFFu;
-  uint32_t px0 = w.px[0], px1 = w.px[1], px2 = w.px[2];
-  int32_t r2 = sp_r, c2 = sp_c;
-  if (s2 != s) {
-    const uint32_t word2 = __ldg(bank + s2);
-    r2 = sp_row(word2);
-    c2 = sp_col(word2);
-    const SpWindow w2 = gather_window(bank, count, sorted, r2, c2);
-    px0 = w2.px[0];
-    px1 = w2.px[1];
-    px2 = w2.px[2];
-  }
-#pragma unroll
-  for (int half = 0; half < 2; ++half) {
-    const uint32_t nib = half ? code >> 4 : code & 0xFu;
-    if (!nib) continue;
-    ++cands;
-    const uint32_t k = candidate_k(nib) + 2 * half;
-    int32_t xs, ys, np;
-    if (flood_window(px0, px1, px2, r2, c2, k, xs, ys, np)) {
-      if (emit) {
-        const uint32_t cx = xs / np;
-        const uint32_t cy = ys / np;
-        const float fx = xs / static_cast<float>(np) - cx;
-        const float fy = ys / static_cast<float>(np) - cy;
-        pts[n] = place_cluster(g, sensor, cx, cy, fx, fy, cx / kChipColumns);
-      }
-      ++n;
-    }
-  }
-  return n;
+  return lo;
 }
 
-// Bitonic sort of (key, slot) pairs in shared memory by one warp; size is a power of two.
-__device__ __forceinline__ void warp_bitonic_sort(unsigned long long* key, uint16_t* slot, uint32_t size)
+struct DecodeEvent {
+  const uint32_t* ev;       // raw event words
+  uint32_t stage_base;      // first staging slot of the event
+  float4* stage;
+  uint32_t* stage_id;
+};
+
+// Appends one cluster to module m's staging slice: slots [2 * SPs before m, ...).
+__device__ __forceinline__ void stage_cluster(DecodeShared& sh, const DecodeEvent& d, uint32_t m,
+                                              const ClusterPoint& p)
+{
+  const uint32_t slot = atomicAdd(&sh.mod_count[m], 1u);
+  const uint32_t o = d.stage_base + 2 * sh.sp_prefix[4 * m] + slot;
+  const float phi = (m & 1) ? phi_odd_side(p.x, p.y) : phi_even_side(p.x, p.y);
+  d.stage[o] = make_float4(p.x, p.y, p.z, phi);
+  d.stage_id[o] = p.id;
+}
+
+// Flood fill of candidate pixel k of flat SP f and staging of the cluster
+// (MaskedVeloClustering.cu:175-461).
+__device__ __forceinline__ void flood_candidate(DecodeShared& sh, const DecodeEvent& d, const GeometryView& g,
+                                                uint32_t f, uint32_t k)
+{
+  const uint32_t b = bank_of(sh, f);
+  const uint32_t s = f - sh.sp_prefix[b];
+  const uint32_t* bank = d.ev + sh.bank_start[b];
+  const uint32_t count = sh.bank_count[b];
+  const bool sorted = !((sh.unsorted[b >> 5] >> (b & 31)) & 1u);
+  // The reference packs the SP index into a u8 when it decodes candidates
+  // (MaskedVeloClustering.cu:179), so above 255 SPs the flood runs on SP s & 0xFF.
+  const uint32_t word2 = __ldg(bank + (s & 0xFFu));
+  const int32_t r2 = sp_row(word2), c2 = sp_col(word2);
+  const SpWindow w = gather_window(bank, count, sorted, r2, c2);
+  int32_t xs, ys, np;
+  if (!flood_window(w.px[0], w.px[1], w.px[2], r2, c2, k, xs, ys, np)) return;
+  const uint32_t cx = xs / np;
+  const uint32_t cy = ys / np;
+  const float fx = xs / static_cast<float>(np) - cx;
+  const float fy = ys / static_cast<float>(np) - cy;
+  stage_cluster(sh, d, b >> 2, place_cluster(g, sh.bank_sensor[b], cx, cy, fx, fy, cx / kChipColumns));
+}
+
+// Sort key of a staged cluster: phi (orderable bits), LHCb id within the module (20 bits:
+// sensor in module, chip, column, row), staging slot (12 bits).
+__device__ __forceinline__ unsigned long long cluster_key(const float4* src, const uint32_t* src_id, uint32_t i)
+{
+  return (static_cast<unsigned long long>(orderable(src[i].w)) << 32) |
+         (static_cast<unsigned long long>(src_id[i] & 0xFFFFFu) << 12) | i;
+}
+
+// Bitonic sort of 32 * 4 keys held 4 per lane (element j * 32 + lane), first `size`
+// elements (a power of two, 32..128).
+__device__ __forceinline__ void warp_register_sort(unsigned long long (&key)[4], uint32_t size)
+{
+  const uint32_t lane = lane_id();
+  const uint32_t per = size >> 5;
+  for (uint32_t k = 2; k <= size; k <<= 1) {
+    for (uint32_t d = k >> 1; d > 0; d >>= 1) {
+      if (d >= 32) {
+        const uint32_t dj = d >> 5;
+#pragma unroll
+        for (uint32_t j = 0; j < 4; ++j) {
+          if (j >= per || (j & dj)) continue;
+          const uint32_t jj = j | dj;
+          const bool up = ((j * 32 + lane) & k) == 0;
+          const unsigned long long a = key[j], b = key[jj];
+          if ((a > b) == up) {
+            key[j] = b;
+            key[jj] = a;
+          }
+        }
+      } else {
+#pragma unroll
+        for (uint32_t j = 0; j < 4; ++j) {
+          if (j >= per) continue;
+          const unsigned long long p = __shfl_xor_sync(0xFFFFFFFFu, key[j], d);
+          const bool lower = (lane & d) == 0;
+          const bool up = ((j * 32 + lane) & k) == 0;
+          key[j] = (lower == up) ? min(key[j], p) : max(key[j], p);
+        }
+      }
+    }
+  }
+}
+
+// Bitonic sort of `size` keys (power of two) in shared memory by one warp.
+__device__ __forceinline__ void warp_smem_sort(unsigned long long* key, uint32_t size)
 {
   const uint32_t lane = lane_id();
   for (uint32_t k = 2; k <= size; k <<= 1) {
@@ -258,13 +279,9 @@ __device__ __forceinline__ void warp_bitonic_sort(unsigned long long* key, uint1
         const uint32_t ixj = i ^ j;
         if (ixj > i) {
           const unsigned long long a = key[i], b = key[ixj];
-          const bool ascending = (i & k) == 0;
-          if ((a > b) == ascending) {
+          if ((a > b) == ((i & k) == 0)) {
             key[i] = b;
             key[ixj] = a;
-            const uint16_t t = slot[i];
-            slot[i] = slot[ixj];
-            slot[ixj] = t;
           }
         }
       }
@@ -277,8 +294,11 @@ template<int W>
 __global__ void __launch_bounds__(W * 32) decode_cluster_sort_kernel(ChainPointers P)
 {
   __shared__ DecodeShared sh;
-  __shared__ unsigned long long s_key[W][kSortCap];
-  __shared__ uint16_t s_slot[W][kSortCap];
+  // the candidate list and the per-warp sort buffers are never live together
+  __shared__ union {
+    uint32_t cand[kCandCap];
+    unsigned long long key[W][kSortCap];
+  } su;
   const uint32_t warp = threadIdx.x >> 5, lane = lane_id();
   const GeometryView g = geometry_view(P.k.geometry);
 
@@ -287,9 +307,10 @@ __global__ void __launch_bounds__(W * 32) decode_cluster_sort_kernel(ChainPointe
       sh.event = atomicAdd(P.queue + 0, 1u);
       sh.flags = 0;
       sh.n_candidates = 0;
+      sh.n_list = 0;
     }
     if (threadIdx.x < (kSensors + 31) / 32) sh.unsorted[threadIdx.x] = 0;
-    if (threadIdx.x < kModules) sh.mod_fill[threadIdx.x] = 0;
+    if (threadIdx.x < kModules) sh.mod_count[threadIdx.x] = 0;
     __syncthreads();
     const uint32_t e = sh.event;
     if (e >= P.n_events) break;
@@ -299,7 +320,8 @@ __global__ void __launch_bounds__(W * 32) decode_cluster_sort_kernel(ChainPointe
     const uint64_t words = bytes / 4;
     const uint32_t header = 2 + kSensors;  // number_of_raw_banks + raw_bank_offset[209]
     // ---- validate the raw event and index its banks ----
-    const bool bad_header = (off & 3) || words < header + 1 || __ldg(ev) != kSensors;
+    const bool bad_header = (off & 3) || words < header + 1 || off / 4 + words > P.hit_capacity ||
+                            __ldg(ev) != kSensors;
     if (!bad_header) {
       const uint64_t payload_bytes = (words - header) * 4;
       for (uint32_t b = threadIdx.x; b < kSensors; b += blockDim.x) {
@@ -327,7 +349,7 @@ __global__ void __launch_bounds__(W * 32) decode_cluster_sort_kernel(ChainPointe
     const bool event_ok = !(sh.flags & kStatusBadRawEvent);
     if (!event_ok)
       for (uint32_t b = threadIdx.x; b <= kSensors; b += blockDim.x) sh.sp_prefix[b] = 0;
-    // ---- bank prefix (warp 0) and sortedness of each bank (all threads) ----
+    // ---- bank prefix (warp 0) and sortedness of each bank ----
     if (event_ok) {
       if (warp == 0) {
         uint32_t carry = 0;
@@ -356,20 +378,58 @@ __global__ void __launch_bounds__(W * 32) decode_cluster_sort_kernel(ChainPointe
     }
     __syncthreads();
     const uint32_t total_sp = sh.sp_prefix[kSensors];
-    // ---- count pass ----
-    if (threadIdx.x < kModules) sh.mod_count[threadIdx.x] = 0;
-    __syncthreads();
+    const uint32_t base = static_cast<uint32_t>(off / 4);
+    const DecodeEvent d{ev, 2 * base, P.stage.xyzp, P.stage.id};
+    // ---- pass 1: isolated SPs, candidate search of the others ----
     uint32_t my_cands = 0;
     for (uint32_t f = threadIdx.x; f < total_sp; f += blockDim.x) {
-      uint32_t b, cands;
-      const uint32_t n = sp_clusters<false>(sh, ev, P, g, f, b, cands, nullptr);
-      if (n) atomicAdd(&sh.mod_count[b >> 2], n);
-      my_cands += cands;
+      const uint32_t b = bank_of(sh, f);
+      const uint32_t s = f - sh.sp_prefix[b];
+      const uint32_t* bank = ev + sh.bank_start[b];
+      const uint32_t word = __ldg(bank + s);
+      const uint32_t sp = sp_mask(word);
+      const int32_t sp_r = sp_row(word), sp_c = sp_col(word);
+      if (sp_isolated(word)) {
+        // pattern table (MaskedVeloClustering.cu:105-167)
+        const uint32_t idx = __ldg(P.k.sp_patterns + sp);
+        const uint32_t chip = sp_c / (kChipColumns / 2);
+        const uint32_t sensor = sh.bank_sensor[b];
+        for (int c = 0; c < 2; ++c) {
+          if (c == 1 && !(idx & 8)) break;
+          const uint32_t row = c ? (idx >> 4) & 3u : idx & 0x03u;
+          const uint32_t col = c ? (idx >> 6) & 1u : (idx >> 2) & 1u;
+          const uint32_t cx = sp_c * 2 + col;
+          const uint32_t cy = sp_r * 4 + row;
+          const float fx = __ldg(P.k.sp_fx + sp * 2 + c);
+          const float fy = __ldg(P.k.sp_fy + sp * 2 + c);
+          stage_cluster(sh, d, b >> 2, place_cluster(g, sensor, cx, cy, fx, fy, chip));
+        }
+        continue;
+      }
+      const bool sorted = !((sh.unsorted[b >> 5] >> (b & 31)) & 1u);
+      const uint32_t code = window_candidate_code(sp, gather_window(bank, sh.bank_count[b], sorted, sp_r, sp_c));
+      for (int half = 0; half < 2; ++half) {
+        const uint32_t nib = half ? code >> 4 : code & 0xFu;
+        if (!nib) continue;
+        ++my_cands;
+        const uint32_t k = candidate_k(nib) + 2 * half;
+        const uint32_t slot = atomicAdd(&sh.n_list, 1u);
+        if (slot < kCandCap) su.cand[slot] = (f << 4) | k;
+        else flood_candidate(sh, d, g, f, k);
+      }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) my_cands += __shfl_xor_sync(0xFFFFFFFFu, my_cands, o);
     if (lane == 0 && my_cands) atomicAdd(&sh.n_candidates, my_cands);
     __syncthreads();
+    // ---- pass 2: flood fill of the listed candidates ----
+    const uint32_t n_list = min(sh.n_list, kCandCap);
+    for (uint32_t i = threadIdx.x; i < n_list; i += blockDim.x) {
+      const uint32_t c = su.cand[i];
+      flood_candidate(sh, d, g, c >> 4, c & 0xFu);
+    }
+    __syncthreads();
+    // ---- compact layout: exclusive scan of the module counts ----
     if (warp == 0) {
       const uint32_t a = lane < kModules ? sh.mod_count[lane] : 0;
       const uint32_t a2 = lane + 32 < kModules ? sh.mod_count[lane + 32] : 0;
@@ -389,64 +449,59 @@ __global__ void __launch_bounds__(W * 32) decode_cluster_sort_kernel(ChainPointe
       if (lane == 0) {
         uint32_t fl = 0;
         // the event's hit region is its raw word range: one hit per raw word
-        if (total > words || off / 4 + total > P.hit_capacity) fl |= kStatusHitOverflow;
+        if (total > words) fl |= kStatusHitOverflow;
         if (sh.n_candidates > kMaxCandidatesEvent) fl |= kStatusCandidateOverflow;
         if (fl) atomicOr(&sh.flags, fl);
       }
     }
     __syncthreads();
-    const uint32_t base = static_cast<uint32_t>(off / 4);
     const bool write = event_ok && !(sh.flags & kStatusHitOverflow);
-    // ---- emit pass: clusters into their module slice (slot order arbitrary) ----
-    if (write) {
-      for (uint32_t f = threadIdx.x; f < total_sp; f += blockDim.x) {
-        uint32_t b, cands;
-        ClusterPoint pts[2];
-        const uint32_t n = sp_clusters<true>(sh, ev, P, g, f, b, cands, pts);
-        if (!n) continue;
-        const uint32_t m = b >> 2;
-        const uint32_t slot = atomicAdd(&sh.mod_fill[m], n);
-        const bool odd = m & 1;
-        for (uint32_t c = 0; c < n; ++c) {
-          const uint32_t o = base + sh.mod_start[m] + slot + c;
-          P.hits.x[o] = pts[c].x;
-          P.hits.y[o] = pts[c].y;
-          P.hits.z[o] = pts[c].z;
-          P.hits.phi[o] = odd ? phi_odd_side(pts[c].x, pts[c].y) : phi_even_side(pts[c].x, pts[c].y);
-          P.hits.id[o] = pts[c].id;
-        }
-      }
-    }
-    __syncthreads();
-    // ---- per-module sort on (phi, LHCb id), in place ----
+    // ---- per-module sort on (phi, LHCb id) into the compact layout ----
     for (uint32_t m = warp; m < kModules; m += W) {
       const uint32_t n = write ? sh.mod_count[m] : 0;
       const uint32_t p0 = base + sh.mod_start[m];
+      const float4* src = d.stage + d.stage_base + 2 * sh.sp_prefix[4 * m];
+      const uint32_t* src_id = d.stage_id + d.stage_base + 2 * sh.sp_prefix[4 * m];
+      float4* dst = P.hits.xyzp + p0;
+      uint32_t* dst_id = P.hits.id + p0;
       if (n > kMaxHitsPerModule && lane == 0) atomicOr(&sh.flags, kStatusModuleOverflow);
-      if (n > 1 && n <= kSortCap) {
-        uint32_t size = 2;
+      if (n <= kRegSortMax) {
+        uint32_t size = 32;
         while (size < n) size <<= 1;
-        for (uint32_t i = lane; i < size; i += 32) {
+        unsigned long long key[4];
+#pragma unroll
+        for (uint32_t j = 0; j < 4; ++j) {
+          const uint32_t i = j * 32 + lane;
+          key[j] = i < n ? cluster_key(src, src_id, i) : ~0ull;
+        }
+        if (n > 1) warp_register_sort(key, size);
+#pragma unroll
+        for (uint32_t j = 0; j < 4; ++j) {
+          const uint32_t i = j * 32 + lane;
           if (i < n) {
-            s_key[warp][i] = (static_cast<unsigned long long>(orderable(P.hits.phi[p0 + i])) << 32) | P.hits.id[p0 + i];
-            s_slot[warp][i] = static_cast<uint16_t>(i);
-          } else {
-            s_key[warp][i] = ~0ull;
-            s_slot[warp][i] = 0;
+            const uint32_t from = static_cast<uint32_t>(key[j] & 0xFFFu);
+            dst[i] = src[from];
+            dst_id[i] = src_id[from];
           }
         }
+      } else if (n <= kSortCap) {
+        unsigned long long* key = su.key[warp];
+        uint32_t size = 256;
+        while (size < n) size <<= 1;
+        for (uint32_t i = lane; i < size; i += 32) key[i] = i < n ? cluster_key(src, src_id, i) : ~0ull;
         __syncwarp();
-        warp_bitonic_sort(s_key[warp], s_slot[warp], size);
-        // the keys are dead after the sort: their buffer stages the permutation
-        uint32_t* tmp = reinterpret_cast<uint32_t*>(s_key[warp]);
-        float* fields_f[4] = {P.hits.x, P.hits.y, P.hits.z, P.hits.phi};
-#pragma unroll 1
-        for (int a = 0; a < 5; ++a) {
-          uint32_t* arr = a < 4 ? reinterpret_cast<uint32_t*>(fields_f[a]) : P.hits.id;
-          for (uint32_t i = lane; i < n; i += 32) tmp[i] = arr[p0 + s_slot[warp][i]];
-          __syncwarp();
-          for (uint32_t i = lane; i < n; i += 32) arr[p0 + i] = tmp[i];
-          __syncwarp();
+        warp_smem_sort(key, size);
+        for (uint32_t i = lane; i < n; i += 32) {
+          const uint32_t from = static_cast<uint32_t>(key[i] & 0xFFFu);
+          dst[i] = src[from];
+          dst_id[i] = src_id[from];
+        }
+        __syncwarp();
+      } else {
+        // beyond the reference's 500-cluster module buffer (flagged above): kept unsorted
+        for (uint32_t i = lane; i < n; i += 32) {
+          dst[i] = src[i];
+          dst_id[i] = src_id[i];
         }
       }
       if (lane == 0) {
@@ -456,9 +511,13 @@ __global__ void __launch_bounds__(W * 32) decode_cluster_sort_kernel(ChainPointe
     }
     __syncthreads();
     if (threadIdx.x == 0) {
+      const uint32_t nhits = write ? sh.mod_start[kModules - 1] + sh.mod_count[kModules - 1] : 0;
       P.event_hit_base[e] = base;
-      P.event_hits[e] = write ? sh.mod_start[kModules - 1] + sh.mod_count[kModules - 1] : 0;
+      P.event_hits[e] = nhits;
       P.status[e] = sh.flags;
+      // route the event to the search mapping chosen for its size
+      if (nhits > P.block_threshold) P.block_events[atomicAdd(P.queue + 5, 1u)] = e;
+      else P.warp_events[atomicAdd(P.queue + 4, 1u)] = e;
     }
     __syncthreads();
   }

@@ -25,7 +25,7 @@ namespace velo {
 // ---------------------------------------------------------------------------
 // Capacities of this implementation
 // ---------------------------------------------------------------------------
-constexpr uint32_t kEventHitCap = 32768;         // hits per event in the search (used bitmask)
+constexpr uint32_t kEventHitCap = 16384;         // hits per event in the search (used bitmask)
 constexpr uint32_t kWeakCap = 4096;              // weak tracklets kept per event
 constexpr uint32_t kTrackletRing = kTtfModulo;   // tracklet ring (reference ring size)
 constexpr uint32_t kStatusEmptyModuleRead = 1u << 10;  // forwarding into an empty module
@@ -40,11 +40,10 @@ struct DeviceConstants {
   const float* sp_fy;         // [512]
 };
 
-struct HitsSoA {
-  float* x;
-  float* y;
-  float* z;
-  float* phi;
+// Clusters after the phi sort: position and phi of a cluster in one 16-byte record (one
+// 128-bit load in the search), LHCb id alongside.
+struct HitsAoS {
+  float4* xyzp;  // x, y, z, phi
   uint32_t* id;
 };
 
@@ -64,7 +63,8 @@ struct ChainPointers {
   uint32_t n_events;
   DeviceConstants k;
   // clusters
-  HitsSoA hits;
+  HitsAoS hits;
+  HitsAoS stage;           // unsorted clusters, per module (capacity 2 per SP word)
   uint32_t* module_start;  // [N*52] absolute
   uint32_t* module_num;    // [N*52]
   uint32_t* event_hit_base;// [N] absolute index of the event's first hit
@@ -84,8 +84,12 @@ struct ChainPointers {
   uint32_t max_tracks_total;
   uint32_t max_track_hits_total;
   uint64_t hit_capacity;       // entries of the hit SoA arrays
-  // work queues
-  uint32_t* queue;             // [4] counters (decode, search)
+  // work queues: [0] decode, [1] warp search, [2] block search, [4] / [5] sizes of the
+  // warp / block event lists
+  uint32_t* queue;             // [8]
+  uint32_t* warp_events;       // [N] events routed to the warp-per-event search
+  uint32_t* block_events;      // [N] events routed to the block-per-event search
+  uint32_t block_threshold;    // events with more clusters than this go to the block search
   // learned pruning (nullptr: plain search)
   const void* mlp;
 };
@@ -186,6 +190,41 @@ __device__ __forceinline__ int window_second(const float* a, uint32_t size, floa
   }
   return fabsf(value - a[l]) < margin ? l + 1 : l;
 }
+// The same two searches over the phi lane (.w) of the float4 cluster records.
+__device__ __forceinline__ int window_first4(const float4* a, uint32_t size, float value, float margin)
+{
+  bool found = false;
+  int l = 0, r = static_cast<int>(size) - 1;
+  while (l < r) {
+    const int m = (l + r) / 2;
+    const float e = a[m].w;
+    found |= fabsf(value - e) < margin;
+    if (value - margin > e) l = m + 1; else r = m;
+  }
+  found |= fabsf(value - a[l].w) < margin;
+  return found ? l : -1;
+}
+__device__ __forceinline__ int window_second4(const float4* a, uint32_t size, float value, float margin)
+{
+  int l = 0, r = static_cast<int>(size) - 1;
+  while (l < r) {
+    const int m = (l + r) / 2;
+    if (value + margin > a[m].w) l = m + 1; else r = m;
+  }
+  return fabsf(value - a[l].w) < margin ? l + 1 : l;
+}
+__device__ __forceinline__ void phi_window4(const float4* H, uint32_t start, uint32_t num, float value, float margin,
+                                            int& first, int& last)
+{
+  first = window_first4(H + start, num, value, margin);
+  last = -1;
+  if (first != -1) {
+    const int s = window_second4(H + start + first, num - first, value, margin);
+    first += start;
+    last = s == 0 ? first + 1 : first + s;
+  }
+}
+
 // [first, last) of hits in a phi-sorted module within margin of value; first = -1 if none.
 __device__ __forceinline__ void phi_window(const float* phis, uint32_t start, uint32_t num, float value, float margin,
                                            int& first, int& last)

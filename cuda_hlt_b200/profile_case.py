@@ -1,0 +1,33 @@
+"""Small fixed workload for profiler captures: one batch of nu ~ U(2,15) events, run
+`--runs` times through the chain (device-resident input, no graphs).
+
+python -m cuda_hlt_b200.profile_case [--events 8192] [--runs 2] [--mode plain]
+"""
+import argparse
+
+import numpy as np
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--events", type=int, default=8192)
+    ap.add_argument("--runs", type=int, default=2)
+    ap.add_argument("--config", default="batched_500k")
+    args = ap.parse_args()
+    import torch
+    from cuda_hlt_b200 import chain, events
+    b = events.generate_config(args.config, n_events=args.events, with_mc=False)
+    raw = torch.from_numpy(b.raw).cuda()
+    off = torch.from_numpy(b.offsets.view(np.int64)).cuda()
+    vc = chain.VeloChain(max_events=args.events, max_raw_bytes=int(b.raw.size) + 4096, max_tracks=160 * args.events,
+                         max_track_hits=12 * 160 * args.events)
+    s = torch.cuda.current_stream().cuda_stream
+    for _ in range(args.runs):
+        vc.run_device(raw.data_ptr(), off.data_ptr(), args.events, s)
+    t, h, c = vc.sync()
+    vc.close()
+    print(f"profile_case: {args.events} events, {c} clusters, {t} tracks, {h} track hits, {b.raw.size} raw bytes")
+
+
+if __name__ == "__main__":
+    main()

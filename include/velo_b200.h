@@ -148,7 +148,7 @@ typedef struct VeloConfig {
  *                        c11,c31,c33,chi2,z [T] each, then bool backward[T]
  * Cluster container after the phi sort (for parity checks and downstream use):
  *   module_hit_start[N*52], module_hit_num[N*52] (starts are absolute indices; gaps allowed),
- *   hit_x/y/z/phi/id indexed by those starts. */
+ *   hit_xyzp (4 floats per cluster: x, y, z, phi) and hit_id indexed by those starts. */
 typedef struct VeloOutputs {
   uint32_t n_events;
   uint32_t* atomics;
@@ -159,10 +159,7 @@ typedef struct VeloOutputs {
   uint32_t* status;
   uint32_t* module_hit_start;
   uint32_t* module_hit_num;
-  float* hit_x;
-  float* hit_y;
-  float* hit_z;
-  float* hit_phi;
+  float* hit_xyzp;
   uint32_t* hit_id;
   uint64_t hit_capacity;
 } VeloOutputs;
@@ -199,6 +196,11 @@ int velo_destroy(VeloCtx* ctx);
 int velo_download(VeloCtx* ctx, void* dst_host, const void* src_device, size_t bytes);
 /* Asynchronous variant on `stream` (dst_host should be pinned). */
 int velo_download_async(VeloCtx* ctx, void* dst_host, const void* src_device, size_t bytes, void* stream);
+
+/* Search mapping: events with more than `clusters` clusters run the block-per-event search,
+ * the others the warp-per-event search (0: all block, >= 16384: all warp). Set by the
+ * autotuner (cuda_hlt_b200/autotune.py) from timings per hit-count bucket. */
+int velo_set_block_threshold(VeloCtx* ctx, uint32_t clusters);
 
 /* Kernel launch count of the last run (all kernels of this library). */
 int velo_last_launch_count(VeloCtx* ctx, uint32_t* n);

@@ -215,3 +215,26 @@ def test_full_size_batch_properties():
     for k in pu.STATE_KEYS:
         assert np.all(np.isfinite(res["states"][k]))
     assert (res["status"] & chain.STATUS["bad_raw"]).sum() == 0
+
+
+@pytest.mark.parametrize("mapping", [chain.MAP_WARP, chain.MAP_BLOCK])
+def test_search_mappings_bit_exact(mapping):
+    """Warp-per-event and block-per-event searches give the reference's result each."""
+    g = load_golden("batched")
+    b = golden_batch("batched")
+    res = run_chain(b, mapping=mapping)
+    N = b.n_events
+    for e in range(N):
+        if res["status"][e] & chain.REFERENCE_UNDEFINED:
+            continue
+        mt, gt = chain.event_tracks(res, e), golden_event_tracks(g, e)
+        assert pu.canonical_tracks(mt) == pu.canonical_tracks(gt), (mapping, e)
+        assert_states_equal(res, e, mt, g, gt, int(g["atomics"][N + e]), (mapping, e))
+
+
+def test_mappings_identical_on_uneven_batch():
+    b = events.generate_config("batched_500k", n_events=400, first_event=3000)
+    outs = [run_chain(b, mapping=m) for m in (chain.MAP_WARP, chain.MAP_BLOCK, chain.MAP_AUTO)]
+    for r in outs[1:]:
+        for e in range(b.n_events):
+            assert pu.canonical_tracks(chain.event_tracks(outs[0], e)) == pu.canonical_tracks(chain.event_tracks(r, e))
