@@ -320,8 +320,9 @@ __global__ void __launch_bounds__(W * 32) decode_cluster_sort_kernel(ChainPointe
     const uint64_t words = bytes / 4;
     const uint32_t header = 2 + kSensors;  // number_of_raw_banks + raw_bank_offset[209]
     // ---- validate the raw event and index its banks ----
-    const bool bad_header = (off & 3) || words < header + 1 || off / 4 + words > P.hit_capacity ||
-                            __ldg(ev) != kSensors;
+    // a batch may start anywhere in the caller's buffer: check the address itself
+    const bool bad_header = (reinterpret_cast<uintptr_t>(ev) & 3) || words < header + 1 ||
+                            off / 4 + words > P.hit_capacity || __ldg(ev) != kSensors;
     if (!bad_header) {
       const uint64_t payload_bytes = (words - header) * 4;
       for (uint32_t b = threadIdx.x; b < kSensors; b += blockDim.x) {

@@ -152,6 +152,24 @@ def test_host_and_device_input_paths_agree():
         assert np.array_equal(ref[k], res[k]), k
 
 
+@pytest.mark.parametrize("shift", [4, 8, 12])
+def test_batch_at_unaligned_address(shift):
+    """A batch may start anywhere (4-byte aligned) inside the caller's buffer."""
+    import torch
+    b = events.generate_config("plain_1k", n_events=40, first_event=7)
+    ref = run_chain(b)
+    buf = torch.zeros(b.raw.size + 64, dtype=torch.uint8, device="cuda")
+    buf[shift:shift + b.raw.size] = torch.from_numpy(b.raw).cuda()
+    off = torch.from_numpy(b.offsets.view(np.int64)).cuda()
+    vc = chain.VeloChain(max_events=40, max_raw_bytes=int(b.raw.size) + 64, use_graphs=True)
+    vc.run_device(buf.data_ptr() + shift, off.data_ptr(), 40, torch.cuda.current_stream().cuda_stream)
+    vc.sync()
+    res = vc.results()
+    vc.close()
+    for k in ("atomics", "track_hit_number", "hit_id", "module_num", "cluster_id", "status"):
+        assert np.array_equal(ref[k], res[k]), k
+
+
 def _empty_event():
     nb = 208
     payload, offs = [], [0]
