@@ -105,6 +105,7 @@ GPU_SYMBOLS = [
     "velo_download_async",
     "velo_set_block_threshold",
     "velo_last_launch_count",
+    "velo_search_static",
     "velo_version",
 ]
 
@@ -173,6 +174,8 @@ def gpu_lib():
         lib.velo_set_block_threshold.restype = C.c_int
         lib.velo_last_launch_count.argtypes = [P, C.POINTER(C.c_uint32)]
         lib.velo_last_launch_count.restype = C.c_int
+        lib.velo_search_static.argtypes = [P] * 4 + [C.c_uint32] + [P] * 5
+        lib.velo_search_static.restype = C.c_int
         lib.velo_version.argtypes = []
         lib.velo_version.restype = C.c_char_p
         _gpu = lib

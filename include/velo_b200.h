@@ -205,6 +205,21 @@ int velo_set_block_threshold(VeloCtx* ctx, uint32_t clusters);
 /* Kernel launch count of the last run (all kernels of this library). */
 int velo_last_launch_count(VeloCtx* ctx, uint32_t* n);
 
+/* Search without allocation, for callers that cannot allocate device memory (for example a
+ * host framework that reserves the device up front and hands out fixed slices). No
+ * counterpart in the reference. Runs search_by_triplet on a cluster container produced by
+ * velo_run (VeloOutputs hit_xyzp, module_hit_start, module_hit_num, status) and writes the
+ * tracks of each event in the reference's Velo::TrackHits terms: track_n[n * 1200] hit
+ * counts and track_hits[n * 1200 * 26] event-relative hit indices, event_tracks[n] and
+ * status_out[n]. Its scratch is a fixed ~23 MB __device__ array, resident on every device
+ * that loads the library: at most 512 events per call (more: VELO_ERR_CAPACITY), all calls
+ * share it (calls overlapping on a device race), and the first call on a device looks up
+ * its address, so that first call should come before any stream capture. Calls no
+ * allocator. */
+int velo_search_static(const float* hit_xyzp, const uint32_t* module_hit_start, const uint32_t* module_hit_num,
+                       const uint32_t* status_in, uint32_t n_events, uint16_t* track_n, uint16_t* track_hits,
+                       uint32_t* event_tracks, uint32_t* status_out, void* stream);
+
 const char* velo_version(void);
 
 #ifdef __cplusplus
