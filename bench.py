@@ -132,13 +132,23 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
+TRAFFIC_SUMMARIES = ["velo_chain_batched_8192_warp_ncu.md", "velo_chain_batched_8192_block1536_ncu.md"]
+
+
 def load_traffic():
-    """DRAM bytes per event of each kernel from the committed ncu summary, if present."""
-    try:
-        with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
-            return json.load(f)
-    except Exception:
-        return None
+    """DRAM bytes per event of each kernel from the first committed ncu summary that
+    holds them (the ```json block of the summary), if present."""
+    merged = {}
+    for name in TRAFFIC_SUMMARIES:
+        try:
+            with open(os.path.join(ROOT, "profiles", name)) as f:
+                text = f.read()
+            block = text.split("```json", 1)[1].split("```", 1)[0]
+            for k, v in json.loads(block).get("bytes_per_event", {}).items():
+                merged.setdefault(k, v)
+        except (OSError, IndexError, ValueError):
+            continue
+    return {"bytes_per_event": merged} if merged else None
 
 
 # ---------------------------------------------------------------------------

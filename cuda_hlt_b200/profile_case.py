@@ -1,7 +1,11 @@
 """Small fixed workload for profiler captures: one batch of nu ~ U(2,15) events, run
 `--runs` times through the chain (device-resident input, no graphs).
 
-python -m cuda_hlt_b200.profile_case [--events 8192] [--runs 2] [--mode plain]
+python -m cuda_hlt_b200.profile_case [--events 8192] [--runs 2] [--block-threshold N]
+
+--block-threshold: events with more clusters than N use the block-per-event search, the
+others the warp-per-event one (1536 is the context default; 16384 sends every event to
+the warp search).
 """
 import argparse
 
@@ -13,6 +17,7 @@ def main():
     ap.add_argument("--events", type=int, default=8192)
     ap.add_argument("--runs", type=int, default=2)
     ap.add_argument("--config", default="batched_500k")
+    ap.add_argument("--block-threshold", type=int, default=1536)
     args = ap.parse_args()
     import torch
     from cuda_hlt_b200 import chain, events
@@ -21,6 +26,7 @@ def main():
     off = torch.from_numpy(b.offsets.view(np.int64)).cuda()
     vc = chain.VeloChain(max_events=args.events, max_raw_bytes=int(b.raw.size) + 4096, max_tracks=160 * args.events,
                          max_track_hits=12 * 160 * args.events)
+    vc.set_block_threshold(args.block_threshold)
     s = torch.cuda.current_stream().cuda_stream
     for _ in range(args.runs):
         vc.run_device(raw.data_ptr(), off.data_ptr(), args.events, s)
