@@ -63,6 +63,20 @@ class VeloConfig(C.Structure):
     ]
 
 
+class VeloMlpWeights(C.Structure):
+    _fields_ = [
+        ("mean", C.c_float * 12),
+        ("inv_std", C.c_float * 12),
+        ("w1", (C.c_float * 13) * 64),
+        ("w2", (C.c_float * 65) * 64),
+        ("w3", (C.c_float * 65) * 2),
+        ("seed_threshold", C.c_float),
+        ("ext_threshold", C.c_float),
+        ("max_event_clusters", C.c_uint32),
+        ("reserved", C.c_uint32),
+    ]
+
+
 class VeloOutputs(C.Structure):
     _fields_ = [
         ("n_events", C.c_uint32),
@@ -77,6 +91,8 @@ class VeloOutputs(C.Structure):
         ("hit_xyzp", C.c_void_p),
         ("hit_id", C.c_void_p),
         ("hit_capacity", C.c_uint64),
+        ("hit_size", C.c_void_p),
+        ("hit_keep", C.c_void_p),
     ]
 
 
@@ -107,6 +123,17 @@ GPU_SYMBOLS = [
     "velo_last_launch_count",
     "velo_search_static",
     "velo_version",
+    "velo_set_mode",
+    "velo_mlp_trainer_create",
+    "velo_mlp_trainer_destroy",
+    "velo_mlp_collect",
+    "velo_mlp_samples",
+    "velo_mlp_normalize",
+    "velo_mlp_train",
+    "velo_mlp_get_weights",
+    "velo_mlp_set_weights",
+    "velo_mlp_gradient",
+    "velo_mlp_infer",
 ]
 
 _host = None
@@ -178,5 +205,22 @@ def gpu_lib():
         lib.velo_search_static.restype = C.c_int
         lib.velo_version.argtypes = []
         lib.velo_version.restype = C.c_char_p
+        lib.velo_set_mode.argtypes = [P, C.c_uint32]
+        lib.velo_set_mode.restype = C.c_int
+        W = C.POINTER(VeloMlpWeights)
+        lib.velo_mlp_trainer_create.argtypes = [C.c_int, C.c_uint64, C.c_uint64, C.POINTER(P)]
+        lib.velo_mlp_trainer_destroy.argtypes = [P]
+        lib.velo_mlp_collect.argtypes = [P, P, C.POINTER(C.c_uint64)]
+        lib.velo_mlp_samples.argtypes = [P, C.c_uint64, C.c_uint32, P, P]
+        lib.velo_mlp_normalize.argtypes = [P]
+        lib.velo_mlp_train.argtypes = [P, C.c_uint32, C.c_uint32, C.c_float, C.POINTER(C.c_float)]
+        lib.velo_mlp_get_weights.argtypes = [P, W]
+        lib.velo_mlp_set_weights.argtypes = [P, W]
+        lib.velo_mlp_gradient.argtypes = [P, P, P, C.c_uint32, W, C.POINTER(C.c_float)]
+        lib.velo_mlp_infer.argtypes = [P, P, C.c_uint32, P]
+        for name in ("velo_mlp_trainer_create", "velo_mlp_trainer_destroy", "velo_mlp_collect", "velo_mlp_samples",
+                     "velo_mlp_normalize", "velo_mlp_train", "velo_mlp_get_weights", "velo_mlp_set_weights",
+                     "velo_mlp_gradient", "velo_mlp_infer"):
+            getattr(lib, name).restype = C.c_int
         _gpu = lib
     return _gpu

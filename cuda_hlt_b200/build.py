@@ -48,7 +48,7 @@ def build_host(force=False):
 
 def build_gpu(force=False, verbose_ptxas=False):
     lib = os.path.join(HERE, "libvelo_b200.so")
-    srcs = [os.path.join(CSRC, f) for f in ("velo_chain.cu", "velo_static.cu")]
+    srcs = [os.path.join(CSRC, f) for f in ("velo_chain.cu", "velo_static.cu", "velo_mlp_train.cu")]
     deps = _sources(".cu") + _sources(".cuh") + _sources(".hpp") + [os.path.join(INCLUDE, "velo_b200.h")]
     if force or _newer(lib, deps + [os.path.join(HERE, "libvelo_host.so")]):
         extra = ["-Xptxas", "-v"] if verbose_ptxas else []

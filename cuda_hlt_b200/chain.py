@@ -31,7 +31,7 @@ SEQUENCE = (
     "velo_kalman_fit_t",
 )
 
-STAGES = ("decode_cluster_sort", "search_by_triplet", "event_scan", "consolidate_fit")
+STAGES = ("decode_cluster_sort", "fill_candidates", "search_by_triplet", "event_scan", "consolidate_fit")
 MODE_PLAIN, MODE_PRUNED = 0, 1
 MAP_AUTO, MAP_BLOCK, MAP_WARP = 0, 1, 2
 N_MODULES = 52
@@ -118,11 +118,20 @@ class VeloChain:
     def stage_times(self):
         """Device milliseconds per stage, summed over the launch sequences recorded since
         set_timing(True); 'runs' is the number of sequences summed."""
-        ms = (C.c_float * 5)()
-        _check(self.lib.velo_stage_times(self.ctx, ms, 5), "velo_stage_times")
-        out = dict(zip(STAGES, list(ms)[:4]))
-        out["runs"] = int(ms[4])
+        n = len(STAGES)
+        ms = (C.c_float * (n + 1))()
+        _check(self.lib.velo_stage_times(self.ctx, ms, n + 1), "velo_stage_times")
+        out = dict(zip(STAGES, list(ms)[:n]))
+        out["runs"] = int(ms[n])
         return out
+
+    def set_mode(self, mode):
+        """MODE_PLAIN (reference semantics) or MODE_PRUNED (learned scorer, set_mlp first)."""
+        _check(self.lib.velo_set_mode(self.ctx, int(mode)), "velo_set_mode")
+
+    def set_mlp(self, weights):
+        """Loads a VeloMlpWeights (see cuda_hlt_b200.mlp) for the pruned mode."""
+        _check(self.lib.velo_set_mlp(self.ctx, C.byref(weights), C.sizeof(weights)), "velo_set_mlp")
 
     def set_block_threshold(self, clusters):
         """Events above `clusters` clusters use the block-per-event search, others the warp one."""
@@ -165,6 +174,9 @@ class VeloChain:
             for i, k in enumerate(("x", "y", "z", "phi")):
                 res["cluster_" + k] = np.ascontiguousarray(xyzp[:, i])
             res["cluster_id"] = self._down(o.hit_id, np.uint32, span)
+            res["cluster_size"] = self._down(o.hit_size, np.uint8, span)
+            if o.hit_keep:
+                res["cluster_keep"] = self._down(o.hit_keep, np.uint8, span)
         return res
 
 
@@ -173,7 +185,7 @@ def event_clusters(res, e):
     out = []
     for m in range(N_MODULES):
         s, n = int(res["module_start"][e * N_MODULES + m]), int(res["module_num"][e * N_MODULES + m])
-        out.append({k: res["cluster_" + k][s:s + n] for k in ("x", "y", "z", "phi", "id")})
+        out.append({k: res["cluster_" + k][s:s + n] for k in ("x", "y", "z", "phi", "id", "size")})
     return out
 
 
@@ -182,3 +194,19 @@ def event_tracks(res, e):
     t0, t1 = int(res["track_offsets"][e]), int(res["track_offsets"][e + 1])
     thn, ids = res["track_hit_number"], res["hit_id"]
     return [tuple(int(v) for v in ids[thn[t]:thn[t + 1]]) for t in range(t0, t1)]
+
+
+def check_tracks(batch, res):
+    """MC-truth efficiency and ghost rate of the tracks in `res` (VeloChain.results()) against
+    the batch's MC_info blobs, with the reference's VELO checker categories
+    (checker/tracking/src/TrackChecker.cpp:349-405): VeloCheckResult."""
+    lib = _lib.host_lib()
+    if batch.mc is None:
+        raise VeloError("batch has no MC truth")
+    evt = np.ascontiguousarray(res["track_offsets"], np.uint32)
+    tho = np.ascontiguousarray(res["track_hit_number"], np.uint32)
+    ids = np.ascontiguousarray(res["hit_id"], np.uint32)
+    out = _lib.VeloCheckResult()
+    _check(lib.velo_check_tracks(batch.mc.ctypes.data, batch.mc_offsets.ctypes.data, batch.n_events, evt.ctypes.data,
+                                 tho.ctypes.data, ids.ctypes.data, C.byref(out)), "velo_check_tracks")
+    return out

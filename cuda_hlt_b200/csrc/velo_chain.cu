@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <array>
@@ -11,7 +12,9 @@
 #include "../../include/velo_b200.h"
 #include "velo_kernels.cuh"
 
+#include "velo_ctx.hpp"
 #include "velo_decode.cuh"
+#include "velo_fill.cuh"
 #include "velo_search.cuh"
 #include "velo_search_block.cuh"
 #include "velo_consolidate.cuh"
@@ -31,6 +34,13 @@ struct VeloCtx {
   uint8_t* d_sp_patterns = nullptr;
   float* d_sp_fx = nullptr;
   float* d_sp_fy = nullptr;
+  uint8_t* d_sp_sizes = nullptr;
+  // learned scorer
+  __nv_bfloat16* d_mlp_w = nullptr;
+  float* d_mlp_norm = nullptr;
+  MlpDevice mlp{};
+  bool mlp_loaded = false;
+  uint32_t mode = VELO_MODE_PLAIN;
   // input staging (for velo_run_host)
   uint8_t* d_raw = nullptr;
   uint64_t* d_raw_offsets = nullptr;
@@ -39,6 +49,9 @@ struct VeloCtx {
   uint32_t* d_hid = nullptr;
   float4* d_stage_xyzp = nullptr;
   uint32_t* d_stage_id = nullptr;
+  uint8_t* d_hit_size = nullptr;
+  uint2* d_windows = nullptr;
+  uint8_t* d_keep = nullptr;
   uint64_t hit_capacity = 0;
   uint32_t *d_module_start = nullptr, *d_module_num = nullptr, *d_event_hit_base = nullptr, *d_event_hits = nullptr,
            *d_status = nullptr;
@@ -55,15 +68,16 @@ struct VeloCtx {
   uint32_t last_n = 0;
   uint32_t launches = 0;
   bool timing = false;
-  // Stage timing: one set of 5 events per launch sequence; a graph keeps the set it was
-  // captured with, plain launches cycle through the sets.
-  std::vector<std::array<cudaEvent_t, 5>> ev_sets;
+  // Stage timing: one set of kStageEvents events per launch sequence; a graph keeps the set
+  // it was captured with, plain launches cycle through the sets.
+  static constexpr int kStageEvents = 6;
+  std::vector<std::array<cudaEvent_t, kStageEvents>> ev_sets;
   std::vector<uint8_t> ev_used;
   uint32_t ev_next = 0;
   int ev_current = -1;
   int decode_warps = 8;
   int search_wpb = 4;
-  uint32_t decode_blocks = 0, search_blocks = 0, search_block_blocks = 0;
+  uint32_t decode_blocks = 0, search_blocks = 0, search_block_blocks = 0, fill_blocks = 0, fill_pruned_blocks = 0;
   // CUDA graphs per (n_events, raw, offsets)
   struct GraphKey {
     uint32_t n;
@@ -107,7 +121,8 @@ cudaError_t dalloc(T*& p, size_t count)
 
 void free_all(VeloCtx* c)
 {
-  void* ptrs[] = {c->d_geometry, c->d_sp_patterns, c->d_sp_fx, c->d_sp_fy, c->d_raw, c->d_raw_offsets, c->d_hxyzp,
+  void* ptrs[] = {c->d_geometry, c->d_sp_patterns, c->d_sp_fx, c->d_sp_fy, c->d_sp_sizes, c->d_mlp_w, c->d_mlp_norm,
+                  c->d_hit_size, c->d_windows, c->d_keep, c->d_raw, c->d_raw_offsets, c->d_hxyzp,
                   c->d_hid, c->d_stage_xyzp, c->d_stage_id, c->d_module_start, c->d_module_num, c->d_event_hit_base,
                   c->d_event_hits, c->d_status, c->d_track_n, c->d_track_hits, c->d_tracklets, c->d_weak, c->d_ttf,
                   c->d_event_tracks, c->d_event_track_hits, c->d_atomics, c->d_track_hit_number,
@@ -127,7 +142,7 @@ constexpr uint32_t kPlainEventSets = 8;
 
 int add_event_set(VeloCtx* c)
 {
-  std::array<cudaEvent_t, 5> set{};
+  std::array<cudaEvent_t, VeloCtx::kStageEvents> set{};
   for (auto& e : set)
     if (cudaEventCreate(&e) != cudaSuccess) return VELO_ERR_CUDA;
   c->ev_sets.push_back(set);
@@ -141,7 +156,8 @@ ChainPointers pointers(VeloCtx* c, const void* raw, const uint64_t* offsets, uin
   P.raw = static_cast<const uint8_t*>(raw);
   P.raw_offsets = offsets;
   P.n_events = n;
-  P.k = DeviceConstants{reinterpret_cast<const float*>(c->d_geometry), c->d_sp_patterns, c->d_sp_fx, c->d_sp_fy};
+  P.k = DeviceConstants{reinterpret_cast<const float*>(c->d_geometry), c->d_sp_patterns, c->d_sp_fx, c->d_sp_fy,
+                        c->d_sp_sizes};
   P.hits = HitsAoS{c->d_hxyzp, c->d_hid};
   P.stage = HitsAoS{c->d_stage_xyzp, c->d_stage_id};
   P.module_start = c->d_module_start;
@@ -149,6 +165,9 @@ ChainPointers pointers(VeloCtx* c, const void* raw, const uint64_t* offsets, uin
   P.event_hit_base = c->d_event_hit_base;
   P.event_hits = c->d_event_hits;
   P.status = c->d_status;
+  P.hit_size = c->d_hit_size;
+  P.windows = c->d_windows;
+  P.keep = c->mode == VELO_MODE_PRUNED ? c->d_keep : nullptr;
   P.scratch = SearchScratch{c->d_track_n, c->d_track_hits, c->d_tracklets, c->d_ttf, c->d_weak};
   P.event_tracks = c->d_event_tracks;
   P.event_track_hits = c->d_event_track_hits;
@@ -165,7 +184,7 @@ ChainPointers pointers(VeloCtx* c, const void* raw, const uint64_t* offsets, uin
   P.warp_events = c->d_warp_events;
   P.block_events = c->d_block_events;
   P.block_threshold = c->block_threshold;
-  P.mlp = nullptr;
+  P.mlp = c->mlp;
   return P;
 }
 
@@ -192,6 +211,14 @@ int launch_chain(VeloCtx* c, const ChainPointers& P, cudaStream_t s, bool captur
     ++c->launches;
   }
   if (c->timing && c->ev_current >= 0) VCK(record(c->ev_sets[c->ev_current][1], s, capturing));
+  if (P.keep) {
+    fill_candidates_kernel<true><<<std::min<uint32_t>(n, c->fill_pruned_blocks), kMlpTile, kFillPrunedSmem, s>>>(P);
+  } else {
+    fill_candidates_kernel<false><<<std::min<uint32_t>(n, c->fill_blocks), kMlpTile, 0, s>>>(P);
+  }
+  VCK(cudaGetLastError());
+  ++c->launches;
+  if (c->timing && c->ev_current >= 0) VCK(record(c->ev_sets[c->ev_current][2], s, capturing));
   {
     // both mappings: each kernel drains its own event list (routed by the decode kernel)
     if (c->block_threshold > 0) {
@@ -207,16 +234,24 @@ int launch_chain(VeloCtx* c, const ChainPointers& P, cudaStream_t s, bool captur
       ++c->launches;
     }
   }
-  if (c->timing && c->ev_current >= 0) VCK(record(c->ev_sets[c->ev_current][2], s, capturing));
+  if (c->timing && c->ev_current >= 0) VCK(record(c->ev_sets[c->ev_current][3], s, capturing));
   event_scan_kernel<<<1, 1024, 0, s>>>(P);
   VCK(cudaGetLastError());
   ++c->launches;
-  if (c->timing && c->ev_current >= 0) VCK(record(c->ev_sets[c->ev_current][3], s, capturing));
+  if (c->timing && c->ev_current >= 0) VCK(record(c->ev_sets[c->ev_current][4], s, capturing));
   consolidate_fit_kernel<4><<<(n + 3) / 4, 128, 0, s>>>(P);
   VCK(cudaGetLastError());
   ++c->launches;
-  if (c->timing && c->ev_current >= 0) VCK(record(c->ev_sets[c->ev_current][4], s, capturing));
+  if (c->timing && c->ev_current >= 0) VCK(record(c->ev_sets[c->ev_current][5], s, capturing));
   return 0;
+}
+
+void drop_graphs(VeloCtx* c)
+{
+  cudaSetDevice(c->device);
+  cudaDeviceSynchronize();
+  for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second.exec);
+  c->graphs.clear();
 }
 
 }  // namespace
@@ -252,12 +287,18 @@ int velo_create(const VeloConfig* cfg, const void* geometry, size_t geometry_byt
   ok &= dalloc(c->d_sp_patterns, 256) == cudaSuccess;
   ok &= dalloc(c->d_sp_fx, 512) == cudaSuccess;
   ok &= dalloc(c->d_sp_fy, 512) == cudaSuccess;
+  ok &= dalloc(c->d_sp_sizes, 256) == cudaSuccess;
+  ok &= dalloc(c->d_mlp_w, kMlpParams) == cudaSuccess;
+  ok &= dalloc(c->d_mlp_norm, 32) == cudaSuccess;
   ok &= dalloc(c->d_raw, cfg->max_raw_bytes + 16) == cudaSuccess;
   ok &= dalloc(c->d_raw_offsets, N + 1) == cudaSuccess;
   ok &= dalloc(c->d_hxyzp, c->hit_capacity) == cudaSuccess;
   ok &= dalloc(c->d_hid, c->hit_capacity) == cudaSuccess;
   ok &= dalloc(c->d_stage_xyzp, 2 * c->hit_capacity) == cudaSuccess;
   ok &= dalloc(c->d_stage_id, 2 * c->hit_capacity) == cudaSuccess;
+  ok &= dalloc(c->d_hit_size, c->hit_capacity) == cudaSuccess;
+  ok &= dalloc(c->d_windows, c->hit_capacity) == cudaSuccess;
+  ok &= dalloc(c->d_keep, c->hit_capacity) == cudaSuccess;
   ok &= dalloc(c->d_module_start, static_cast<size_t>(N) * kModules) == cudaSuccess;
   ok &= dalloc(c->d_module_num, static_cast<size_t>(N) * kModules) == cudaSuccess;
   ok &= dalloc(c->d_event_hit_base, N) == cudaSuccess;
@@ -287,7 +328,8 @@ int velo_create(const VeloConfig* cfg, const void* geometry, size_t geometry_byt
   if (cudaMemcpy(c->d_geometry, geometry, kGeometryBytes, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(c->d_sp_patterns, pat, 256, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(c->d_sp_fx, fx, sizeof fx, cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy(c->d_sp_fy, fy, sizeof fy, cudaMemcpyHostToDevice) != cudaSuccess)
+      cudaMemcpy(c->d_sp_fy, fy, sizeof fy, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(c->d_sp_sizes, sizes, 256, cudaMemcpyHostToDevice) != cudaSuccess)
     return fail(VELO_ERR_CUDA);
   int occ = 0;
   if (c->decode_warps == 8)
@@ -301,6 +343,14 @@ int velo_create(const VeloConfig* cfg, const void* geometry, size_t geometry_byt
                        static_cast<int>(kStageCap * sizeof(float4)));
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, search_block_kernel, kBlockThreads, kStageCap * sizeof(float4));
   c->search_block_blocks = static_cast<uint32_t>(std::max(1, occ) * c->sm_count);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fill_candidates_kernel<false>, kMlpTile, 0);
+  c->fill_blocks = static_cast<uint32_t>(std::max(1, occ) * c->sm_count);
+  // the pruned form holds 64 tensor-memory columns per CTA: at most 8 CTAs per SM
+  cudaFuncSetAttribute(fill_candidates_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       static_cast<int>(kFillPrunedSmem));
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fill_candidates_kernel<true>, kMlpTile, kFillPrunedSmem);
+  c->fill_pruned_blocks = static_cast<uint32_t>(std::min(std::max(1, occ), 8) * c->sm_count);
+  c->mode = cfg->mode == VELO_MODE_PRUNED ? VELO_MODE_PRUNED : VELO_MODE_PLAIN;
   // mapping: VELO_MAP_WARP keeps every event on warps, VELO_MAP_BLOCK on blocks; the
   // default splits at a cluster count (velo_set_block_threshold / the autotuner move it)
   c->block_threshold = cfg->mapping == VELO_MAP_WARP ? kEventHitCap : (cfg->mapping == VELO_MAP_BLOCK ? 0u : 1536u);
@@ -325,6 +375,8 @@ static int fill_outputs(VeloCtx* c, uint32_t n, VeloOutputs* out)
   out->hit_xyzp = reinterpret_cast<float*>(c->d_hxyzp);
   out->hit_id = c->d_hid;
   out->hit_capacity = c->hit_capacity;
+  out->hit_size = c->d_hit_size;
+  out->hit_keep = c->mode == VELO_MODE_PRUNED ? c->d_keep : nullptr;
   return 0;
 }
 
@@ -333,6 +385,7 @@ int velo_run(VeloCtx* c, const void* raw, const uint64_t* raw_offsets, uint32_t 
 {
   if (!c || (!raw && n_events) || (!raw_offsets && n_events)) return VELO_ERR_INVALID;
   if (n_events > c->cfg.max_events) return VELO_ERR_CAPACITY;
+  if (c->mode == VELO_MODE_PRUNED && !c->mlp_loaded) return VELO_ERR_STATE;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (cudaSetDevice(c->device) != cudaSuccess) return VELO_ERR_CUDA;
   c->last_stream = s;
@@ -420,7 +473,9 @@ int velo_sync(VeloCtx* c, uint32_t* total_tracks, uint32_t* total_track_hits, ui
     VCK(cudaMemcpyAsync(c->h_totals, c->d_atomics + 2 * N, 4, cudaMemcpyDeviceToHost, s));
     VCK(cudaMemcpyAsync(c->h_totals + 1, c->d_event_hit_offset + N, 4, cudaMemcpyDeviceToHost, s));
   }
+  VCK(cudaMemcpyAsync(c->h_totals + 2, c->d_queue + 6, 4, cudaMemcpyDeviceToHost, s));
   VCK(cudaStreamSynchronize(s));
+  if (c->h_totals[2]) return VELO_ERR_DEVICE_TIMEOUT;
   if (total_tracks) *total_tracks = c->h_totals[0];
   if (total_track_hits) *total_track_hits = c->h_totals[1];
   if (total_clusters) {
@@ -435,8 +490,43 @@ int velo_sync(VeloCtx* c, uint32_t* total_tracks, uint32_t* total_track_hits, ui
 
 int velo_set_mlp(VeloCtx* c, const void* weights_host, size_t bytes)
 {
-  if (!c || !weights_host || bytes == 0) return VELO_ERR_INVALID;
-  return VELO_ERR_STATE;
+  if (!c || !weights_host || bytes != sizeof(VeloMlpWeights)) return VELO_ERR_INVALID;
+  const VeloMlpWeights& w = *static_cast<const VeloMlpWeights*>(weights_host);
+  if (!(w.seed_threshold > 0.f && w.seed_threshold < 1.f) || !(w.ext_threshold >= 0.f && w.ext_threshold < 1.f))
+    return VELO_ERR_INVALID;
+  // bf16 slots: W1 [64][16], W2 [64][80], W3 [16][80], bias in the ones column, zero pads
+  std::vector<__nv_bfloat16> slots(kMlpParams, __float2bfloat16_rn(0.f));
+  for (int j = 0; j < 64; ++j)
+    for (int i = 0; i < 13; ++i) slots[j * kMlpK1 + i] = __float2bfloat16_rn(w.w1[j][i]);
+  for (int j = 0; j < 64; ++j)
+    for (int i = 0; i < 65; ++i) slots[kMlpW1 + j * kMlpK2 + i] = __float2bfloat16_rn(w.w2[j][i]);
+  for (int o = 0; o < 2; ++o)
+    for (int i = 0; i < 65; ++i) slots[kMlpW1 + kMlpW2 + o * kMlpK2 + i] = __float2bfloat16_rn(w.w3[o][i]);
+  float norm[32] = {};
+  for (int k = 0; k < 12; ++k) {
+    norm[k] = w.mean[k];
+    norm[16 + k] = w.inv_std[k];
+  }
+  drop_graphs(c);  // the launch parameters change
+  VCK(cudaMemcpy(c->d_mlp_w, slots.data(), kMlpParams * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice));
+  VCK(cudaMemcpy(c->d_mlp_norm, norm, sizeof norm, cudaMemcpyHostToDevice));
+  auto logit = [](float p) { return std::log(p / (1.f - p)); };
+  c->mlp.w = c->d_mlp_w;
+  c->mlp.norm = c->d_mlp_norm;
+  c->mlp.seed_logit = logit(w.seed_threshold);
+  c->mlp.use_ext = w.ext_threshold > 0.f ? 1u : 0u;
+  c->mlp.ext_logit = w.ext_threshold > 0.f ? logit(w.ext_threshold) : 0.f;
+  c->mlp.max_hits = w.max_event_clusters;
+  c->mlp_loaded = true;
+  return 0;
+}
+
+int velo_set_mode(VeloCtx* c, uint32_t mode)
+{
+  if (!c || (mode != VELO_MODE_PLAIN && mode != VELO_MODE_PRUNED)) return VELO_ERR_INVALID;
+  if (mode != c->mode) drop_graphs(c);
+  c->mode = mode;
+  return 0;
 }
 
 int velo_set_timing(VeloCtx* c, int enabled)
@@ -452,25 +542,26 @@ int velo_set_timing(VeloCtx* c, int enabled)
   return 0;
 }
 
-// Sums, over every event set recorded since velo_set_timing, the device time of the four
-// stages; ms[4] (when n > 4) receives the number of launch sequences summed.
+// Sums, over every event set recorded since velo_set_timing, the device time of the five
+// stages; ms[5] (when n > 5) receives the number of launch sequences summed.
 int velo_stage_times(VeloCtx* c, float* ms, int n)
 {
-  if (!c || !ms || n < 4) return VELO_ERR_INVALID;
+  constexpr int kStages = VeloCtx::kStageEvents - 1;
+  if (!c || !ms || n < kStages) return VELO_ERR_INVALID;
   if (c->ev_sets.empty()) return VELO_ERR_STATE;
-  float acc[4] = {0.f, 0.f, 0.f, 0.f};
+  float acc[kStages] = {};
   int runs = 0;
   for (size_t k = 0; k < c->ev_sets.size(); ++k) {
     if (!c->ev_used[k]) continue;
-    for (int i = 0; i < 4; ++i) {
+    for (int i = 0; i < kStages; ++i) {
       float t = 0.f;
       VCK(cudaEventElapsedTime(&t, c->ev_sets[k][i], c->ev_sets[k][i + 1]));
       acc[i] += t;
     }
     ++runs;
   }
-  for (int i = 0; i < 4; ++i) ms[i] = acc[i];
-  if (n > 4) ms[4] = static_cast<float>(runs);
+  for (int i = 0; i < kStages; ++i) ms[i] = acc[i];
+  if (n > kStages) ms[kStages] = static_cast<float>(runs);
   return 0;
 }
 
@@ -495,13 +586,7 @@ int velo_download_async(VeloCtx* c, void* dst_host, const void* src_device, size
 int velo_set_block_threshold(VeloCtx* c, uint32_t clusters)
 {
   if (!c) return VELO_ERR_INVALID;
-  if (clusters != c->block_threshold) {
-    // the launch sequence changes: drop captured graphs
-    cudaSetDevice(c->device);
-    cudaDeviceSynchronize();
-    for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second.exec);
-    c->graphs.clear();
-  }
+  if (clusters != c->block_threshold) drop_graphs(c);  // the launch sequence changes
   c->block_threshold = clusters;
   return 0;
 }
@@ -524,3 +609,12 @@ int velo_destroy(VeloCtx* c)
 }
 
 }  // extern "C"
+
+bool velo_ctx_last_run(VeloCtx* c, ChainPointers* P, cudaStream_t* stream, int* device)
+{
+  if (!c || !P || c->last_n == 0) return false;
+  *P = pointers(c, nullptr, nullptr, c->last_n);
+  *stream = c->last_stream;
+  *device = c->device;
+  return true;
+}

@@ -191,15 +191,21 @@ struct DecodeEvent {
   uint32_t* stage_id;
 };
 
-// Appends one cluster to module m's staging slice: slots [2 * SPs before m, ...).
+// Bits 26-27 of an LHCb VP id are always zero (sensor < 208 ends at bit 25): the staging
+// record carries the cluster's pixel count there, at most 3.
+constexpr uint32_t kSizeShift = 26;
+constexpr uint32_t kSizeMask = 3u << kSizeShift;
+
+// Appends one cluster of `pixels` pixels to module m's staging slice: slots
+// [2 * SPs before m, ...).
 __device__ __forceinline__ void stage_cluster(DecodeShared& sh, const DecodeEvent& d, uint32_t m,
-                                              const ClusterPoint& p)
+                                              const ClusterPoint& p, uint32_t pixels)
 {
   const uint32_t slot = atomicAdd(&sh.mod_count[m], 1u);
   const uint32_t o = d.stage_base + 2 * sh.sp_prefix[4 * m] + slot;
   const float phi = (m & 1) ? phi_odd_side(p.x, p.y) : phi_even_side(p.x, p.y);
   d.stage[o] = make_float4(p.x, p.y, p.z, phi);
-  d.stage_id[o] = p.id;
+  d.stage_id[o] = p.id | (min(pixels, 3u) << kSizeShift);
 }
 
 // Flood fill of candidate pixel k of flat SP f and staging of the cluster
@@ -223,7 +229,8 @@ __device__ __forceinline__ void flood_candidate(DecodeShared& sh, const DecodeEv
   const uint32_t cy = ys / np;
   const float fx = xs / static_cast<float>(np) - cx;
   const float fy = ys / static_cast<float>(np) - cy;
-  stage_cluster(sh, d, b >> 2, place_cluster(g, sh.bank_sensor[b], cx, cy, fx, fy, cx / kChipColumns));
+  stage_cluster(sh, d, b >> 2, place_cluster(g, sh.bank_sensor[b], cx, cy, fx, fy, cx / kChipColumns),
+                static_cast<uint32_t>(np));
 }
 
 // Sort key of a staged cluster: phi (orderable bits), LHCb id within the module (20 bits:
@@ -403,7 +410,8 @@ __global__ void __launch_bounds__(W * 32) decode_cluster_sort_kernel(ChainPointe
           const uint32_t cy = sp_r * 4 + row;
           const float fx = __ldg(P.k.sp_fx + sp * 2 + c);
           const float fy = __ldg(P.k.sp_fy + sp * 2 + c);
-          stage_cluster(sh, d, b >> 2, place_cluster(g, sensor, cx, cy, fx, fy, chip));
+          stage_cluster(sh, d, b >> 2, place_cluster(g, sensor, cx, cy, fx, fy, chip),
+                        (__ldg(P.k.sp_sizes + sp) >> (4 * c)) & 0xFu);
         }
         continue;
       }
@@ -465,6 +473,7 @@ __global__ void __launch_bounds__(W * 32) decode_cluster_sort_kernel(ChainPointe
       const uint32_t* src_id = d.stage_id + d.stage_base + 2 * sh.sp_prefix[4 * m];
       float4* dst = P.hits.xyzp + p0;
       uint32_t* dst_id = P.hits.id + p0;
+      uint8_t* dst_size = P.hit_size + p0;
       if (n > kMaxHitsPerModule && lane == 0) atomicOr(&sh.flags, kStatusModuleOverflow);
       if (n <= kRegSortMax) {
         uint32_t size = 32;
@@ -481,8 +490,10 @@ __global__ void __launch_bounds__(W * 32) decode_cluster_sort_kernel(ChainPointe
           const uint32_t i = j * 32 + lane;
           if (i < n) {
             const uint32_t from = static_cast<uint32_t>(key[j] & 0xFFFu);
+            const uint32_t id = src_id[from];
             dst[i] = src[from];
-            dst_id[i] = src_id[from];
+            dst_id[i] = id & ~kSizeMask;
+            dst_size[i] = static_cast<uint8_t>(id >> kSizeShift) & 3u;
           }
         }
       } else if (n <= kSortCap) {
@@ -494,15 +505,18 @@ __global__ void __launch_bounds__(W * 32) decode_cluster_sort_kernel(ChainPointe
         warp_smem_sort(key, size);
         for (uint32_t i = lane; i < n; i += 32) {
           const uint32_t from = static_cast<uint32_t>(key[i] & 0xFFFu);
+          const uint32_t id = src_id[from];
           dst[i] = src[from];
-          dst_id[i] = src_id[from];
+          dst_id[i] = id & ~kSizeMask;
+          dst_size[i] = static_cast<uint8_t>(id >> kSizeShift) & 3u;
         }
         __syncwarp();
       } else {
         // beyond the reference's 500-cluster module buffer (flagged above): kept unsorted
         for (uint32_t i = lane; i < n; i += 32) {
           dst[i] = src[i];
-          dst_id[i] = src_id[i];
+          dst_id[i] = src_id[i] & ~kSizeMask;
+          dst_size[i] = static_cast<uint8_t>(src_id[i] >> kSizeShift) & 3u;
         }
       }
       if (lane == 0) {

@@ -1,12 +1,15 @@
 // Device code of the B200 VELO chain.
 //
-// Four kernels per batch, no host round trip between them:
+// Five kernels per batch, no host round trip between them:
 //   decode_cluster_sort   one block per event (persistent, events pulled from a queue);
 //                         each warp owns whole modules: SuperPixel decode, masked
 //                         clustering, phi, per-module sort, compact SoA write.
-//   search_by_triplet     one warp per event (persistent, queue): seeding with on-the-fly
-//                         phi windows, forwarding, weak-track recovery; hit_used is a
-//                         shared-memory bitmask.
+//   fill_candidates       one block per event (persistent, queue): phi windows of every
+//                         h1; in the pruned mode also the learned seed/extension scores
+//                         (tensor cores).
+//   search_by_triplet     one warp per event (persistent, queue): seeding over the
+//                         precomputed windows, forwarding, weak-track recovery; hit_used
+//                         is a shared-memory bitmask.
 //   event_scan            one block: exclusive scans of tracks and track hits per event.
 //   consolidate_fit       one warp per event: hit gather into the consolidated SoA, the
 //                         beamline least-squares state and the simplified Kalman state.
@@ -15,6 +18,7 @@
 // forwarding fit, fits) keep the reference's operation order so that, compiled with the
 // same --use_fast_math flags, they round identically; the reference line for each is cited.
 #pragma once
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -38,6 +42,17 @@ struct DeviceConstants {
   const uint8_t* sp_patterns; // [256]
   const float* sp_fx;         // [512]
   const float* sp_fy;         // [512]
+  const uint8_t* sp_sizes;    // [256] pixels of the first (low nibble) and second cluster
+};
+
+// Parameters of the learned seed/extension scorer as the kernels read them.
+struct MlpDevice {
+  const __nv_bfloat16* w;  // W1 [64][16], W2 [64][80], W3 [16][80], row-major, bias in the ones column
+  const float* norm;       // feature mean[16], 1/std[16]
+  float seed_logit;        // h1 kept as a seed when logit 0 >= seed_logit
+  float ext_logit;         // hit kept as an extension candidate when logit 1 >= ext_logit
+  uint32_t use_ext;        // extension pruning on
+  uint32_t max_hits;       // events with more clusters fall back to the plain search
 };
 
 // Clusters after the phi sort: position and phi of a cluster in one 16-byte record (one
@@ -70,6 +85,10 @@ struct ChainPointers {
   uint32_t* event_hit_base;// [N] absolute index of the event's first hit
   uint32_t* event_hits;    // [N]
   uint32_t* status;        // [N]
+  uint8_t* hit_size;       // [hit capacity] pixels of each cluster, at most 3
+  // candidates
+  uint2* windows;          // [hit capacity] {h0 first | last << 16, h2 first | last << 16}
+  uint8_t* keep;           // [hit capacity] learned keep bits; nullptr in the plain mode
   // search
   SearchScratch scratch;
   uint32_t* event_tracks;      // [N] tracks per event
@@ -84,14 +103,14 @@ struct ChainPointers {
   uint32_t max_tracks_total;
   uint32_t max_track_hits_total;
   uint64_t hit_capacity;       // entries of the hit SoA arrays
-  // work queues: [0] decode, [1] warp search, [2] block search, [4] / [5] sizes of the
-  // warp / block event lists
+  // work queues: [0] decode, [1] warp search, [2] block search, [3] fill_candidates,
+  // [4] / [5] sizes of the warp / block event lists, [6] error bits
   uint32_t* queue;             // [8]
   uint32_t* warp_events;       // [N] events routed to the warp-per-event search
   uint32_t* block_events;      // [N] events routed to the block-per-event search
   uint32_t block_threshold;    // events with more clusters than this go to the block search
-  // learned pruning (nullptr: plain search)
-  const void* mlp;
+  // learned pruning (read when keep != nullptr)
+  MlpDevice mlp;
 };
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }

@@ -1,9 +1,12 @@
-// Kernel 2 of the chain: search_by_triplet, one warp per event (persistent, queue).
+// Kernel 3 of the chain: search_by_triplet, one warp per event (persistent, queue).
 //
 // The module loop, forwarding and weak-track rules are those of the reference
 // (ProcessModules.cu:8-163, TrackForwarding.cu:41-181, TrackSeeding.cu:7-200,
 // WeakTracksAdder.cu:88-115). What changes is the mapping onto the warp:
-//   * seeding: the h1 candidates of a step are compacted into a shared list, their
+//   * seeding: the phi windows of every h1 come precomputed from fill_candidates (in the
+//     pruned mode only h1 with the learned seed-keep bit are considered, and forwarding
+//     skips candidates without the extension-keep bit when that pruning is on);
+//     the h1 candidates of a step are compacted into a shared list, their
 //     (h1, h0) pairs are flattened over the lanes, and each h1 keeps its best triplet in a
 //     shared 64-bit key (scatter bits, h0 offset, h2 offset) reduced with atomicMin. The
 //     winner is the minimal scatter, first in (h0, h2) order; an atomicMax twin with the
@@ -186,6 +189,9 @@ __global__ void __launch_bounds__(WPB * 32) search_kernel(ChainPointers P)
       }
       __syncwarp();
       const float4* H = P.hits.xyzp + base;
+      const uint2* Wn = P.windows + base;
+      const uint8_t* K = P.keep ? P.keep + base : nullptr;
+      const uint8_t* KE = (P.keep && P.mlp.use_ext) ? P.keep + base : nullptr;  // extension pruning
       uint16_t* track_n = P.scratch.track_n + static_cast<size_t>(e) * kMaxTracks;
       uint16_t* track_hits = P.scratch.track_hits + static_cast<size_t>(e) * kMaxTracks * kMaxTrackSize;
       uint16_t* tracklets = P.scratch.tracklets + static_cast<size_t>(e) * kTrackletRing * 3;
@@ -200,7 +206,6 @@ __global__ void __launch_bounds__(WPB * 32) search_kernel(ChainPointers P)
         for (int side = 2; side <= 3; ++side) {
           const uint32_t m = first - side;
           const uint32_t start = mstart[m], num = mnum[m];
-          const uint32_t m0s = mstart[m + 2], m0n = mnum[m + 2], m2s = mstart[m - 2], m2n = mnum[m - 2];
           for (uint32_t r0 = 0; r0 < num; r0 += kSeedChunk) {
             const uint32_t r_end = min(num, r0 + kSeedChunk);
             // (a) unused h1 with both phi windows (FillCandidates.cu:31-68, TrackSeeding.cu:24-49)
@@ -210,11 +215,13 @@ __global__ void __launch_bounds__(WPB * 32) search_kernel(ChainPointers P)
               const uint32_t h1 = start + r;
               int f0 = -1, l0 = -1, f2 = -1, l2 = -1;
               bool has = false;
-              if (r < r_end && !test_used(used, h1)) {
-                const float p = H[h1].w;
-                if (m0n > 0) phi_window4(H, m0s, m0n, p, kPhiExtrapolation, f0, l0);
-                if (m2n > 0) phi_window4(H, m2s, m2n, p, kPhiExtrapolation, f2, l2);
-                has = f0 != -1 && f2 != -1;
+              if (r < r_end && !test_used(used, h1) && (!K || (K[h1] & 1u))) {
+                const uint2 w = Wn[h1];
+                f0 = static_cast<int>(w.x & 0xFFFFu);
+                l0 = static_cast<int>(w.x >> 16);
+                f2 = static_cast<int>(w.y & 0xFFFFu);
+                l2 = static_cast<int>(w.y >> 16);
+                has = f0 != 0xFFFF && f2 != 0xFFFF;
               }
               uint32_t cnt;
               const uint32_t rank = ballot_rank(has, cnt);
@@ -353,6 +360,7 @@ __global__ void __launch_bounds__(WPB * 32) search_kernel(ChainPointers P)
             const int n_odd = ol - of, n_even = el - ef;
             for (int j = 0; j < n_odd + n_even; ++j) {
               const int h2i = j < n_odd ? of + j : ef + j - n_odd;
+              if (KE && !(KE[h2i] & 2u)) continue;
               const float4 h2 = H[h2i];
               const float dz = h2.z - h0.z;
               const float predx = tx * dz;

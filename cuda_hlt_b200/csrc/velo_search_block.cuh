@@ -186,6 +186,9 @@ __global__ void __launch_bounds__(kBlockThreads) search_block_kernel(ChainPointe
         return;
       }
       const float4* H = staged ? stage : P.hits.xyzp + base;
+      const uint2* Wn = P.windows + base;  // phi windows of every h1 (fill_candidates)
+      const uint8_t* K = P.keep ? P.keep + base : nullptr;
+      const uint8_t* KE = (P.keep && P.mlp.use_ext) ? P.keep + base : nullptr;
       uint16_t* track_n = P.scratch.track_n + static_cast<size_t>(ev) * kMaxTracks;
       uint16_t* track_hits = P.scratch.track_hits + static_cast<size_t>(ev) * kMaxTracks * kMaxTrackSize;
       uint16_t* tracklets = P.scratch.tracklets + static_cast<size_t>(ev) * kTrackletRing * 3;
@@ -208,11 +211,13 @@ __global__ void __launch_bounds__(kBlockThreads) search_block_kernel(ChainPointe
           if (r < total_h1) {
             const uint32_t m = r < na ? ma : mb;
             h1 = mstart[m] + (r < na ? r : r - na);
-            if (!test_used(used, h1)) {
-              const float p = H[h1].w;
-              if (mnum[m + 2] > 0) phi_window4(H, mstart[m + 2], mnum[m + 2], p, kPhiExtrapolation, f0, l0);
-              if (mnum[m - 2] > 0) phi_window4(H, mstart[m - 2], mnum[m - 2], p, kPhiExtrapolation, f2, l2);
-              has = f0 != -1 && f2 != -1;
+            if (!test_used(used, h1) && (!K || (K[h1] & 1u))) {
+              const uint2 w = Wn[h1];
+              f0 = static_cast<int>(w.x & 0xFFFFu);
+              l0 = static_cast<int>(w.x >> 16);
+              f2 = static_cast<int>(w.y & 0xFFFFu);
+              l2 = static_cast<int>(w.y >> 16);
+              has = f0 != 0xFFFF && f2 != 0xFFFF;
             }
           }
           uint32_t rk[3], tot[3];
@@ -330,6 +335,7 @@ __global__ void __launch_bounds__(kBlockThreads) search_block_kernel(ChainPointe
             const int n_odd = ol - of, n_even = el - ef;
             for (int j = 0; j < n_odd + n_even; ++j) {
               const int h2i = j < n_odd ? of + j : ef + j - n_odd;
+              if (KE && !(KE[h2i] & 2u)) continue;
               const float4 h2 = H[h2i];
               const float dz = h2.z - h0.z;
               const float predx = tx * dz;

@@ -48,6 +48,7 @@ extern "C" {
 #define VELO_ERR_BAD_MC -6       /* malformed MC truth blob */
 #define VELO_ERR_NO_DEVICE -7    /* no CUDA device visible */
 #define VELO_ERR_STATE -8        /* call out of order (e.g. pruned run without weights) */
+#define VELO_ERR_DEVICE_TIMEOUT -9 /* a bounded wait in a kernel ran out (tensor core did not answer) */
 
 /* ---- per-event status flags written by velo_run (status[N]) ---- */
 #define VELO_STATUS_BAD_RAW (1u << 0)
@@ -148,7 +149,9 @@ typedef struct VeloConfig {
  *                        c11,c31,c33,chi2,z [T] each, then bool backward[T]
  * Cluster container after the phi sort (for parity checks and downstream use):
  *   module_hit_start[N*52], module_hit_num[N*52] (starts are absolute indices; gaps allowed),
- *   hit_xyzp (4 floats per cluster: x, y, z, phi) and hit_id indexed by those starts. */
+ *   hit_xyzp (4 floats per cluster: x, y, z, phi) and hit_id indexed by those starts,
+ *   hit_size (pixels of each cluster, at most 3) and, in VELO_MODE_PRUNED, hit_keep (the
+ *   scorer's bits per hit: bit 0 seed keep, bit 1 extension keep; NULL in the plain mode). */
 typedef struct VeloOutputs {
   uint32_t n_events;
   uint32_t* atomics;
@@ -162,6 +165,8 @@ typedef struct VeloOutputs {
   float* hit_xyzp;
   uint32_t* hit_id;
   uint64_t hit_capacity;
+  uint8_t* hit_size;
+  uint8_t* hit_keep;
 } VeloOutputs;
 
 /* Creates a context: device buffers for cfg->max_events events, device constants from the
@@ -181,11 +186,65 @@ int velo_run_host(VeloCtx* ctx, const void* raw_host, const uint64_t* raw_offset
 /* Waits for the context's last run; fills totals (tracks, track hits, clusters). */
 int velo_sync(VeloCtx* ctx, uint32_t* total_tracks, uint32_t* total_track_hits, uint64_t* total_clusters);
 
-/* Loads the learned seed/extension scorer (see velo_mlp_*); required for VELO_MODE_PRUNED. */
+/* ---- learned seed/extension scorer (no counterpart in the reference) ----
+ * A 12 -> 64 -> 64 -> 2 MLP scores each seeding candidate h1 of search_by_triplet
+ * (TrackSeeding.cu:7-200) from one proxy triplet: the hits bracketing phi(h1) in its h0
+ * and h2 windows, the pair with the smallest seeding scatter. Features, in order: tx, ty
+ * of h0->h2, log(1 + 1000 * scatter), phi(h0) - phi(h1), phi(h1) - phi(h2), module index,
+ * h0 window size, h2 window size, radius of h1, pixels of h1, h0, h2 (at most 3).
+ * Output 0 ("seed keep") predicts that the plain search keeps h1 on a final track; output
+ * 1 ("extension keep") that h1 is the fourth or a later hit of one. In VELO_MODE_PRUNED the
+ * search seeds only from h1 with p0 >= seed_threshold and, when ext_threshold > 0,
+ * forwards only onto hits with p1 >= ext_threshold; events with more than
+ * max_event_clusters clusters run the plain search (VELO_STATUS_MLP_FALLBACK).
+ * Inference and training run on the tensor cores in bf16 with fp32 accumulation. */
+typedef struct VeloMlpWeights {
+  float mean[12];               /* feature normalisation: (f - mean) * inv_std */
+  float inv_std[12];
+  float w1[64][13];             /* hidden 1 x (12 features, bias) */
+  float w2[64][65];             /* hidden 2 x (64, bias) */
+  float w3[2][65];              /* outputs x (64, bias) */
+  float seed_threshold;         /* probability */
+  float ext_threshold;          /* probability; 0 disables extension pruning */
+  uint32_t max_event_clusters;  /* occupancy limit of the trained range */
+  uint32_t reserved;
+} VeloMlpWeights;
+
+/* Loads the scorer (weights_host -> VeloMlpWeights, bytes == sizeof(VeloMlpWeights));
+ * required before a run in VELO_MODE_PRUNED. */
 int velo_set_mlp(VeloCtx* ctx, const void* weights_host, size_t bytes);
 
-/* Device time of each stage of the last run, milliseconds (decode+cluster+sort, search,
- * scan, consolidate+fit); filled after velo_sync when timing was enabled. */
+/* Switches the context between VELO_MODE_PLAIN and VELO_MODE_PRUNED. */
+int velo_set_mode(VeloCtx* ctx, uint32_t mode);
+
+/* Trainer of the scorer on one device. Samples are the seeding candidates of plain runs,
+ * labelled by the tracks of that run. */
+typedef struct VeloMlpTrainer VeloMlpTrainer;
+int velo_mlp_trainer_create(int device, uint64_t max_samples, uint64_t seed, VeloMlpTrainer** out);
+int velo_mlp_trainer_destroy(VeloMlpTrainer* t);
+/* Appends the candidates of the last velo_run of ctx (plain mode, after velo_sync) until
+ * max_samples are held; *n_total receives the number held. */
+int velo_mlp_collect(VeloMlpTrainer* t, VeloCtx* ctx, uint64_t* n_total);
+/* Copies held samples [first, first+n): features[n][12], label bits[n] (bit 0 seed keep,
+ * bit 1 extension keep). */
+int velo_mlp_samples(VeloMlpTrainer* t, uint64_t first, uint32_t n, float* features, uint8_t* labels);
+/* Sets the feature normalisation from the held samples (mean and 1/std). */
+int velo_mlp_normalize(VeloMlpTrainer* t);
+/* Minibatch Adam (beta 0.9 / 0.999) over the held samples, reshuffled every epoch;
+ * *last_loss = mean cross-entropy of the last epoch. */
+int velo_mlp_train(VeloMlpTrainer* t, uint32_t epochs, uint32_t batch, float lr, float* last_loss);
+int velo_mlp_get_weights(VeloMlpTrainer* t, VeloMlpWeights* w);
+int velo_mlp_set_weights(VeloMlpTrainer* t, const VeloMlpWeights* w);
+/* Gradient of the mean cross-entropy over n host samples at the trainer's weights, from
+ * the training kernels (w1/w2/w3 of *grad; the rest zero). */
+int velo_mlp_gradient(VeloMlpTrainer* t, const float* features, const uint8_t* labels, uint32_t n,
+                      VeloMlpWeights* grad, float* loss);
+/* Logits [n][2] of n host feature rows from the inference kernel code. */
+int velo_mlp_infer(VeloMlpTrainer* t, const float* features, uint32_t n, float* logits);
+
+/* Device time of each stage of the runs recorded since velo_set_timing, milliseconds:
+ * ms[0] decode+cluster+sort, ms[1] fill_candidates (windows, scorer), ms[2] search,
+ * ms[3] scan, ms[4] consolidate+fit, ms[5] (n > 5) number of runs summed. */
 int velo_stage_times(VeloCtx* ctx, float* ms, int n);
 int velo_set_timing(VeloCtx* ctx, int enabled);
 
