@@ -1,16 +1,22 @@
 #!/usr/bin/env python
-"""Throughput of the B200 VELO chain on the 500,000-event nu ~ U(2,15) workload.
+"""Throughput of the B200 VELO chain, MLP-pruned vs plain, on the 1,000,000-event
+nu ~ U(2,20) workload.
 
 python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-One step = one pass of the chain over the rank's 500,000 synthetic events (seed 0,
-events rank*500000 ...), in batches of 16,384 events (one CUDA graph per batch).
-Events are independent, so ranks process disjoint event ranges with no data-path
-collective (weak scaling); NCCL is used only for the barrier and the max over ranks of
-the elapsed device time. Prints one JSON line (rank 0).
-  value   events/s with the raw banks resident in HBM (CUDA events around K steps)
-  e2e     events/s through velo_run_host from pinned host memory, each batch's
-          consolidated tracks and Kalman states read back to pinned host memory
+One step = one pass of the chain over the rank's 1,000,000 synthetic events (seed 4,
+events rank*1000000 ...), in batches of 16,384 events (one CUDA graph per batch). Both
+forms run on the same device-resident input: the plain chain (reference semantics) and
+the pruned chain (learned seed scorer; events above the scorer's trained occupancy fall
+back to the plain search). Events are independent, so ranks process disjoint event
+ranges with no data-path collective (weak scaling); NCCL is used only for the barrier and
+the max over ranks of the elapsed device time. Prints one JSON line (rank 0):
+  value     events/s of the pruned chain, raw banks resident in HBM (CUDA events around
+            K steps); plain.value the same for the plain chain; pruned_vs_plain their ratio
+  quality   long-track efficiency and ghost rate of both forms against generator truth on
+            the head of the workload
+  e2e       events/s of the pruned chain through velo_run_host from pinned host memory,
+            each batch's consolidated tracks and Kalman states read back to pinned memory
   roofline, cpu_baseline, clocks, gpu_launches: see DESIGN.md
 --impl reference times the CPU implementation of the chain (the CPU oracle restating the
 reference kernels; the reference has no CPU tracking) on the host cores, on a bounded
@@ -34,8 +40,8 @@ from cuda_hlt_b200 import chain, events  # noqa: E402
 
 METRIC = "VELO events/s on 1 B200, MLP-pruned vs plain at ≤0.2% eff loss; % HBM peak"
 UNIT = "events/s"
-WORKLOAD = "batched_500k"
-N_EVENTS = 500_000
+WORKLOAD = "pruned_1m"
+N_EVENTS = 1_000_000
 BUCKET = 16384
 CHUNK = 4 * BUCKET
 
@@ -154,49 +160,33 @@ def load_traffic():
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
-def run_ours(args, rank, world, local_rank):
-    import torch
-    import torch.distributed as dist
-
-    torch.cuda.set_device(local_rank)
-    dev = torch.device("cuda", local_rank)
-    threads = max(1, (os.cpu_count() or 1) // max(1, world))
+def load_scorer(args):
+    """The committed scorer weights (trained on the GPU by cuda_hlt_b200.train_scorer), or a
+    scorer trained here with --retrain / when the file is missing."""
+    from cuda_hlt_b200 import mlp, train_scorer
+    path = args.weights or train_scorer.DEFAULT_WEIGHTS
+    if not args.retrain and os.path.exists(path):
+        w = mlp.load_weights(path)
+        return w, {"weights": os.path.relpath(path, ROOT), "trained": "committed", "seed_threshold": w.seed_threshold,
+                   "max_event_clusters": w.max_event_clusters}
+    log("training the scorer (train_scorer pipeline, 1M samples, 4 epochs)")
     t0 = time.time()
-    n_events = args.events
-    chunks = generate_workload(rank * n_events, n_events, threads)
-    log(f"[rank {rank}] generated {n_events} events in {time.time() - t0:.1f}s, "
-        f"{sum(c.raw.size for c in chunks) / 1e9:.2f} GB raw")
-    plan = batch_plan(chunks)
-    max_batch_bytes = max(int(chunks[ci].offsets[b] - chunks[ci].offsets[a]) for ci, a, b in plan)
+    trainer = mlp.MlpTrainer(1_000_000, seed=1)
+    held, max_clusters, _, _ = train_scorer.collect_training(trainer, 1_000_000, os.cpu_count() or 1)
+    trainer.normalize()
+    trainer.train(4, 16384, 2e-3)
+    w = trainer.weights()
+    trainer.close()
+    w.max_event_clusters = max_clusters
+    w.seed_threshold = 0.1
+    w.ext_threshold = 0.0
+    return w, {"trained": f"in bench: {held} samples, {time.time() - t0:.1f}s", "seed_threshold": 0.1,
+               "max_event_clusters": max_clusters}
 
-    # device-resident copy of the raw banks and per-batch offset arrays
-    d_raw = [torch.from_numpy(c.raw).to(dev) for c in chunks]
-    offs_host = []
-    for ci, a, b in plan:
-        o = chunks[ci].offsets[a:b + 1]
-        offs_host.append((o - o[0]).astype(np.uint64))
-    d_offs = [torch.from_numpy(o.view(np.int64)).to(dev) for o in offs_host]
-    batch_ptrs = [(d_raw[ci].data_ptr() + int(chunks[ci].offsets[a]), d_offs[k].data_ptr(), b - a)
-                  for k, (ci, a, b) in enumerate(plan)]
-    stream = torch.cuda.current_stream(dev).cuda_stream
 
-    vc = chain.VeloChain(max_events=BUCKET, max_raw_bytes=max_batch_bytes + 4096, device=local_rank,
-                         use_graphs=True)
-    # search mapping per hit-count bucket, tuned on the first batch (outside the timed region)
-    from cuda_hlt_b200 import autotune
-    threshold, tune_ms = autotune.tune_block_threshold(vc, *batch_ptrs[0], stream)
-    vc.set_timing(True)
-
-    # census: per-batch totals for the algorithmic-byte accounting
-    clusters = tracks = track_hits = 0
-    for raw_p, off_p, n in batch_ptrs:
-        vc.run_device(raw_p, off_p, n, stream)
-        t, h, c = vc.sync()
-        tracks += t
-        track_hits += h
-        clusters += c
-    raw_bytes = sum(int(c.raw.size) for c in chunks)
-
+def time_form(vc, batch_ptrs, stream, args, world, dist, torch, local_rank):
+    """Warm-up, then K timed steps of one form: (elapsed ms, max over ranks; stage times;
+    clocks during the timed region)."""
     def step():
         for raw_p, off_p, n in batch_ptrs:
             vc.run_device(raw_p, off_p, n, stream)
@@ -220,18 +210,19 @@ def run_ours(args, rank, world, local_rank):
         dist.barrier()
     elapsed_ms = start.elapsed_time(end)
     if world > 1:
-        t = torch.tensor([elapsed_ms], device=dev)
+        t = torch.tensor([elapsed_ms], device=torch.device("cuda", local_rank))
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         elapsed_ms = float(t.item())
-    stages = vc.stage_times()
-    n_batches = len(plan)
-    value = n_events * world * args.steps / (elapsed_ms / 1e3)
-    ms_per_step = elapsed_ms / args.steps
+    return elapsed_ms, vc.stage_times(), clocks.summary()
 
-    # ---- roofline of the dominant kernel (per launch = one batch) ----
+
+def roofline(stages, census, n_events, n_batches, peak, peak_kind, traffic_table):
+    """HBM roofline of the dominant kernel of one form (per launch = one batch)."""
+    clusters, tracks, track_hits, raw_bytes = (census[k] for k in ("clusters", "tracks", "track_hits", "raw_bytes"))
     per = {  # algorithmic bytes of one step, per stage
         "decode_cluster_sort": raw_bytes + 16 * clusters,
-        "search_by_triplet": 16 * clusters + 2 * track_hits + 2 * tracks,
+        "fill_candidates": 16 * clusters + 8 * clusters,
+        "search_by_triplet": 16 * clusters + 8 * clusters + 2 * track_hits + 2 * tracks,
         "event_scan": 16 * n_events,
         "consolidate_fit": 34 * track_hits + 98 * tracks + 8 * tracks,
     }
@@ -240,42 +231,145 @@ def run_ours(args, rank, world, local_rank):
     avg_launch_ms = stage_ms[dominant] / max(1, stages["runs"])
     alg_bytes_launch = per[dominant] / n_batches
     achieved = alg_bytes_launch / (avg_launch_ms / 1e3) / 1e9
-    peak, peak_kind = load_peaks()
     traffic = None
-    tr = load_traffic()
-    if tr and dominant in tr.get("bytes_per_event", {}):
-        traffic = tr["bytes_per_event"][dominant] * n_events / n_batches
+    if traffic_table and dominant in traffic_table.get("bytes_per_event", {}):
+        traffic = traffic_table["bytes_per_event"][dominant] * n_events / n_batches
+    return {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "peak_source": peak_kind,
+            "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+            "algorithmic_bytes_per_launch": alg_bytes_launch, "avg_launch_ms": avg_launch_ms,
+            "chain_alg_bytes_per_event": (raw_bytes + 16 * track_hits + 98 * tracks + 4 * (tracks + n_batches)
+                                          + 8 * n_batches) / n_events}, stage_ms
 
-    # ---- end to end through velo_run_host with host buffers ----
-    e2e = run_e2e(args, chunks, plan, local_rank, torch, world, dist, threshold)
 
+def run_quality(weights, n, threads):
+    """Long-track efficiency and ghost rate of both forms against generator truth on the
+    first n events of the workload (with MC truth)."""
+    rows = {"plain": [], "pruned": []}
+    for a in range(0, n, BUCKET):
+        m = min(BUCKET, n - a)
+        b = events.generate_config(WORKLOAD, n_events=m, first_event=a, threads=threads, with_mc=True)
+        for name, mode in (("plain", chain.MODE_PLAIN), ("pruned", chain.MODE_PRUNED)):
+            vc = chain.VeloChain(max_events=m, max_raw_bytes=int(b.raw.size) + 4096)
+            vc.set_mlp(weights)
+            vc.set_mode(mode)
+            vc.run_host(b)
+            vc.sync()
+            res = vc.results(clusters=False)
+            vc.close()
+            c = chain.check_tracks(b, res)
+            rows[name].append((c.long_reconstructible, c.long_found, c.tracks, c.ghosts, c.velo_reconstructible,
+                               c.velo_found))
+    out = {}
+    for name, r in rows.items():
+        lr, lf, t, g, vr, vf = (sum(x[i] for x in r) for i in range(6))
+        out[name] = {"long_efficiency": lf / max(1, lr), "ghost_rate": g / max(1, t), "velo_efficiency": vf / max(1, vr),
+                     "tracks": t, "long_reconstructible": lr}
+    out["events"] = n
+    out["long_efficiency_loss"] = out["plain"]["long_efficiency"] - out["pruned"]["long_efficiency"]
+    out["ghost_rate_change"] = out["pruned"]["ghost_rate"] - out["plain"]["ghost_rate"]
+    return out
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    threads = max(1, (os.cpu_count() or 1) // max(1, world))
+    weights, scorer_info = load_scorer(args)
+    t0 = time.time()
+    n_events = args.events
+    chunks = generate_workload(rank * n_events, n_events, threads)
+    log(f"[rank {rank}] generated {n_events} events in {time.time() - t0:.1f}s, "
+        f"{sum(c.raw.size for c in chunks) / 1e9:.2f} GB raw")
+    plan = batch_plan(chunks)
+    n_batches = len(plan)
+    max_batch_bytes = max(int(chunks[ci].offsets[b] - chunks[ci].offsets[a]) for ci, a, b in plan)
+
+    # device-resident copy of the raw banks and per-batch offset arrays
+    d_raw = [torch.from_numpy(c.raw).to(dev) for c in chunks]
+    offs_host = []
+    for ci, a, b in plan:
+        o = chunks[ci].offsets[a:b + 1]
+        offs_host.append((o - o[0]).astype(np.uint64))
+    d_offs = [torch.from_numpy(o.view(np.int64)).to(dev) for o in offs_host]
+    batch_ptrs = [(d_raw[ci].data_ptr() + int(chunks[ci].offsets[a]), d_offs[k].data_ptr(), b - a)
+                  for k, (ci, a, b) in enumerate(plan)]
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    raw_bytes = sum(int(c.raw.size) for c in chunks)
+    peak, peak_kind = load_peaks()
+    traffic_table = load_traffic()
+    from cuda_hlt_b200 import autotune
+
+    forms = {}
+    for name, mode in (("plain", chain.MODE_PLAIN), ("pruned", chain.MODE_PRUNED)):
+        vc = chain.VeloChain(max_events=BUCKET, max_raw_bytes=max_batch_bytes + 4096, device=local_rank,
+                             use_graphs=True)
+        vc.set_mlp(weights)
+        vc.set_mode(mode)
+        # search mapping per hit-count bucket, tuned on the first batch (outside the timed region)
+        threshold, tune_ms = autotune.tune_block_threshold(vc, *batch_ptrs[0], stream)
+        # census: per-batch totals for the algorithmic-byte accounting and the fallback share
+        census = dict(clusters=0, tracks=0, track_hits=0, raw_bytes=raw_bytes, fallback_events=0)
+        for raw_p, off_p, n in batch_ptrs:
+            vc.run_device(raw_p, off_p, n, stream)
+            t, h, c = vc.sync()
+            census["tracks"] += t
+            census["track_hits"] += h
+            census["clusters"] += c
+            st = np.empty(n, np.uint32)
+            chain._check(vc.lib.velo_download(vc.ctx, st.ctypes.data, chain.C.c_void_p(vc.out.status), 4 * n),
+                         "velo_download")
+            census["fallback_events"] += int(((st & chain.STATUS["mlp_fallback"]) != 0).sum())
+        launches = vc.launch_count()
+        elapsed_ms, stages, clocks = time_form(vc, batch_ptrs, stream, args, world, dist, torch, local_rank)
+        roof, stage_ms = roofline(stages, census, n_events, n_batches, peak, peak_kind, traffic_table)
+        forms[name] = {"value": n_events * world * args.steps / (elapsed_ms / 1e3),
+                       "ms_per_step": elapsed_ms / args.steps,
+                       "stages_ms_per_step": {k: v / args.steps for k, v in stage_ms.items()},
+                       "roofline": roof, "census_per_step": census,
+                       "search_mapping": {"block_above_clusters": threshold,
+                                          "search_ms_per_threshold": {str(k): v for k, v in tune_ms.items()}},
+                       "gpu_launches": launches * n_batches * args.steps, "clocks": clocks, "threshold": threshold}
+        vc.close()
+        log(f"[rank {rank}] {name}: {forms[name]['value']:.0f} events/s")
+
+    # ---- track quality of both forms on the MC-carrying head of the workload ----
+    quality = run_quality(weights, args.quality_events, threads) if rank == 0 and args.quality_events > 0 else None
+
+    # ---- end to end through velo_run_host with host buffers (pruned form) ----
+    e2e = run_e2e(args, chunks, plan, local_rank, torch, world, dist, forms["pruned"]["threshold"], weights)
+
+    p, q = forms["pruned"], forms["plain"]
     result = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
-        "config": {"workload": f"{WORKLOAD}: {n_events} events per GPU, pileup nu ~ U(2,15), seed 0, "
-                               f"events rank*{n_events}...", "events_per_gpu": n_events, "batch_events": BUCKET,
-                   "batches_per_step": n_batches, "mode": "plain", "graphs": True,
-                   "search_mapping": {"block_above_clusters": threshold,
-                                      "search_ms_per_threshold": {str(k): v for k, v in tune_ms.items()}},
+        "metric": METRIC, "value": p["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": p["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "fp32 (scorer: bf16 operands, fp32 accumulation)", "data": "synthetic",
+        "config": {"workload": f"{WORKLOAD}: {n_events} events per GPU, pileup nu ~ U(2,20), seed 4, events "
+                               f"rank*{n_events}..., MLP-pruned search; events above the scorer's trained "
+                               f"occupancy fall back to the plain search", "events_per_gpu": n_events,
+                   "batch_events": BUCKET, "batches_per_step": n_batches, "mode": "pruned", "graphs": True,
+                   "scorer": scorer_info, "search_mapping": p["search_mapping"],
                    "l2": f"inputs larger than L2 ({raw_bytes / 1e9:.2f} GB raw banks per step)",
                    "parallelism": f"event shards x{world}"},
-        "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "peak_source": peak_kind,
-                     "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
-                     "algorithmic_bytes_per_launch": alg_bytes_launch, "avg_launch_ms": avg_launch_ms,
-                     "chain_alg_bytes_per_event": (raw_bytes + 16 * track_hits + 98 * tracks + 4 * (tracks + n_batches)
-                                                   + 8 * n_batches) / n_events},
-        "stages_ms_per_step": stage_ms,
-        "totals_per_step": {"clusters": clusters, "tracks": tracks, "track_hits": track_hits, "raw_bytes": raw_bytes},
+        "roofline": p["roofline"],
+        "stages_ms_per_step": p["stages_ms_per_step"],
+        "totals_per_step": p["census_per_step"],
+        "fallback_fraction": p["census_per_step"]["fallback_events"] / n_events,
+        "plain": {"value": q["value"], "ms_per_step": q["ms_per_step"], "stages_ms_per_step": q["stages_ms_per_step"],
+                  "roofline": q["roofline"], "totals_per_step": q["census_per_step"], "clocks": q["clocks"],
+                  "search_mapping": q["search_mapping"], "gpu_launches": q["gpu_launches"]},
+        "pruned_vs_plain": p["value"] / q["value"],
+        "quality": quality,
         "e2e": e2e,
-        "gpu_launches": 4 * n_batches * args.steps,
-        "clocks": clocks.summary(),
+        "gpu_launches": p["gpu_launches"],
+        "clocks": p["clocks"],
     }
-    vc.close()
     return result, chunks
 
 
-def run_e2e(args, chunks, plan, local_rank, torch, world, dist, threshold):
+def run_e2e(args, chunks, plan, local_rank, torch, world, dist, threshold, weights):
     """velo_run_host from pinned memory, two contexts alternating on two streams so that
     the copies of one batch overlap the kernels of the other; outputs read back to pinned
     host buffers every batch."""
@@ -292,6 +386,8 @@ def run_e2e(args, chunks, plan, local_rank, torch, world, dist, threshold):
             for _ in range(2)]
     for vc in ctxs:
         vc.set_block_threshold(threshold)
+        vc.set_mlp(weights)
+        vc.set_mode(chain.MODE_PRUNED)
     streams = [torch.cuda.Stream(device=local_rank) for _ in range(2)]
     # pinned result buffers per context: atomics, hit numbers, hits SoA, Kalman states
     cap_t = 400 * BUCKET
@@ -427,7 +523,8 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
         "config": {"workload": f"{WORKLOAD}: bounded sample of {sample} events per step (first events of the "
-                               f"500,000-event workload)", "mode": "plain"},
+                               f"1,000,000-event nu ~ U(2,20) workload)",
+                   "mode": "plain (the reference has no learned pruning)"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"{sample} events per step, full chain"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -440,9 +537,12 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--events", type=int, default=N_EVENTS, help="events per GPU (default: the 500,000 workload)")
+    ap.add_argument("--events", type=int, default=N_EVENTS, help="events per GPU (default: the 1,000,000 workload)")
     ap.add_argument("--cpu-sample", type=int, default=16384)
     ap.add_argument("--reference-sample", type=int, default=8192)
+    ap.add_argument("--quality-events", type=int, default=32768, help="MC-checked events of the workload head")
+    ap.add_argument("--weights", default=None, help="scorer weights (default: the committed file)")
+    ap.add_argument("--retrain", action="store_true", help="train the scorer here instead of loading it")
     ap.add_argument("--no-extras", action="store_true", help="skip the CPU baseline and reference-GPU legs")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
