@@ -52,6 +52,8 @@ struct VeloCtx {
   uint8_t* d_hit_size = nullptr;
   uint2* d_windows = nullptr;
   uint8_t* d_keep = nullptr;
+  uint8_t* d_cand_feat = nullptr;
+  uint32_t* d_cand_slot = nullptr;
   uint64_t hit_capacity = 0;
   uint32_t *d_module_start = nullptr, *d_module_num = nullptr, *d_event_hit_base = nullptr, *d_event_hits = nullptr,
            *d_status = nullptr;
@@ -77,7 +79,8 @@ struct VeloCtx {
   int ev_current = -1;
   int decode_warps = 8;
   int search_wpb = 4;
-  uint32_t decode_blocks = 0, search_blocks = 0, search_block_blocks = 0, fill_blocks = 0, fill_pruned_blocks = 0;
+  uint32_t decode_blocks = 0, search_blocks = 0, search_block_blocks = 0, fill_blocks = 0, fill_pruned_blocks = 0,
+           score_blocks = 0;
   // CUDA graphs per (n_events, raw, offsets)
   struct GraphKey {
     uint32_t n;
@@ -122,7 +125,7 @@ cudaError_t dalloc(T*& p, size_t count)
 void free_all(VeloCtx* c)
 {
   void* ptrs[] = {c->d_geometry, c->d_sp_patterns, c->d_sp_fx, c->d_sp_fy, c->d_sp_sizes, c->d_mlp_w, c->d_mlp_norm,
-                  c->d_hit_size, c->d_windows, c->d_keep, c->d_raw, c->d_raw_offsets, c->d_hxyzp,
+                  c->d_hit_size, c->d_windows, c->d_keep, c->d_cand_feat, c->d_cand_slot, c->d_raw, c->d_raw_offsets, c->d_hxyzp,
                   c->d_hid, c->d_stage_xyzp, c->d_stage_id, c->d_module_start, c->d_module_num, c->d_event_hit_base,
                   c->d_event_hits, c->d_status, c->d_track_n, c->d_track_hits, c->d_tracklets, c->d_weak, c->d_ttf,
                   c->d_event_tracks, c->d_event_track_hits, c->d_atomics, c->d_track_hit_number,
@@ -168,6 +171,8 @@ ChainPointers pointers(VeloCtx* c, const void* raw, const uint64_t* offsets, uin
   P.hit_size = c->d_hit_size;
   P.windows = c->d_windows;
   P.keep = c->mode == VELO_MODE_PRUNED ? c->d_keep : nullptr;
+  P.cand_feat = c->d_cand_feat;
+  P.cand_slot = c->d_cand_slot;
   P.scratch = SearchScratch{c->d_track_n, c->d_track_hits, c->d_tracklets, c->d_ttf, c->d_weak};
   P.event_tracks = c->d_event_tracks;
   P.event_track_hits = c->d_event_track_hits;
@@ -212,12 +217,15 @@ int launch_chain(VeloCtx* c, const ChainPointers& P, cudaStream_t s, bool captur
   }
   if (c->timing && c->ev_current >= 0) VCK(record(c->ev_sets[c->ev_current][1], s, capturing));
   if (P.keep) {
-    fill_candidates_kernel<true><<<std::min<uint32_t>(n, c->fill_pruned_blocks), kMlpTile, kFillPrunedSmem, s>>>(P);
+    fill_candidates_kernel<true><<<std::min<uint32_t>(n, c->fill_pruned_blocks), kFillThreads, 0, s>>>(P);
+    VCK(cudaGetLastError());
+    score_candidates_kernel<<<c->score_blocks, kMlpTile, kScoreSmem, s>>>(P);
+    c->launches += 2;
   } else {
-    fill_candidates_kernel<false><<<std::min<uint32_t>(n, c->fill_blocks), kMlpTile, 0, s>>>(P);
+    fill_candidates_kernel<false><<<std::min<uint32_t>(n, c->fill_blocks), kFillThreads, 0, s>>>(P);
+    ++c->launches;
   }
   VCK(cudaGetLastError());
-  ++c->launches;
   if (c->timing && c->ev_current >= 0) VCK(record(c->ev_sets[c->ev_current][2], s, capturing));
   {
     // both mappings: each kernel drains its own event list (routed by the decode kernel)
@@ -299,6 +307,8 @@ int velo_create(const VeloConfig* cfg, const void* geometry, size_t geometry_byt
   ok &= dalloc(c->d_hit_size, c->hit_capacity) == cudaSuccess;
   ok &= dalloc(c->d_windows, c->hit_capacity) == cudaSuccess;
   ok &= dalloc(c->d_keep, c->hit_capacity) == cudaSuccess;
+  ok &= dalloc(c->d_cand_feat, (c->hit_capacity + kMlpTile) * kMlpK1 * 2) == cudaSuccess;
+  ok &= dalloc(c->d_cand_slot, c->hit_capacity) == cudaSuccess;
   ok &= dalloc(c->d_module_start, static_cast<size_t>(N) * kModules) == cudaSuccess;
   ok &= dalloc(c->d_module_num, static_cast<size_t>(N) * kModules) == cudaSuccess;
   ok &= dalloc(c->d_event_hit_base, N) == cudaSuccess;
@@ -343,13 +353,15 @@ int velo_create(const VeloConfig* cfg, const void* geometry, size_t geometry_byt
                        static_cast<int>(kStageCap * sizeof(float4)));
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, search_block_kernel, kBlockThreads, kStageCap * sizeof(float4));
   c->search_block_blocks = static_cast<uint32_t>(std::max(1, occ) * c->sm_count);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fill_candidates_kernel<false>, kMlpTile, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fill_candidates_kernel<false>, kFillThreads, 0);
   c->fill_blocks = static_cast<uint32_t>(std::max(1, occ) * c->sm_count);
-  // the pruned form holds 64 tensor-memory columns per CTA: at most 8 CTAs per SM
-  cudaFuncSetAttribute(fill_candidates_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       static_cast<int>(kFillPrunedSmem));
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fill_candidates_kernel<true>, kMlpTile, kFillPrunedSmem);
-  c->fill_pruned_blocks = static_cast<uint32_t>(std::min(std::max(1, occ), 8) * c->sm_count);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fill_candidates_kernel<true>, kFillThreads, 0);
+  c->fill_pruned_blocks = static_cast<uint32_t>(std::max(1, occ) * c->sm_count);
+  // the scorer holds 64 tensor-memory columns per CTA: at most 8 CTAs per SM
+  cudaFuncSetAttribute(score_candidates_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       static_cast<int>(kScoreSmem));
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, score_candidates_kernel, kMlpTile, kScoreSmem);
+  c->score_blocks = static_cast<uint32_t>(std::min(std::max(1, occ), 8) * c->sm_count);
   c->mode = cfg->mode == VELO_MODE_PRUNED ? VELO_MODE_PRUNED : VELO_MODE_PLAIN;
   // mapping: VELO_MAP_WARP keeps every event on warps, VELO_MAP_BLOCK on blocks; the
   // default splits at a cluster count (velo_set_block_threshold / the autotuner move it)

@@ -1,20 +1,31 @@
 // Kernel 2 of the chain: fill_candidates. For every hit h1 of modules 2..49 the phi windows
 // of h0 (module m+2) and h2 (module m-2) with the reference's searches and tolerance
 // (FillCandidates.cu:8-70, VeloTools.cuh:6-42). The reference computes them in a kernel of
-// their own too; here one 128-thread CTA per event (persistent, queue slot 3) writes them
-// as event-relative u16 pairs {first, last} (0xFFFF = none), so the search kernel reads a
-// window instead of binary-searching inside its serial module loop.
+// their own too; here one thread per hit (a 256-thread CTA per event, persistent, queue slot
+// 3) writes them as event-relative u16 pairs {first, last} (0xFFFF = none), so the search
+// kernel reads a window instead of binary-searching inside its serial module loop.
 //
-// In the pruned mode the same CTA computes the twelve proxy-triplet features of each h1,
-// runs the learned scorer on the tensor cores (128 hits per tile) and writes a keep byte
-// per hit: bit 0 seed keep, bit 1 extension keep. Events above the scorer's occupancy range
-// keep every hit (the plain search) and get VELO_STATUS_MLP_FALLBACK.
+// Pruned mode, two kernels:
+//   fill_candidates<true>  also computes the twelve proxy-triplet features of every seeding
+//                          candidate (both windows non-empty) and appends them, normalised
+//                          and in bf16, to a compact list of 128-row tiles laid out for the
+//                          tensor core (queue slot 7 counts the rows), with the candidate's
+//                          hit slot alongside;
+//   score_candidates       a persistent tcgen05 kernel: each CTA bulk-copies 4 KB tiles of
+//                          that list into shared memory (double-buffered), runs the MLP and
+//                          writes the verdict per candidate: a pruned seed gets its h0 window
+//                          cleared, so the search never sees it; keep bits per hit (bit 0
+//                          seed keep, bit 1 extension keep) are kept for the outputs.
+// Events above the scorer's occupancy range append no candidates (the plain search) and get
+// VELO_STATUS_MLP_FALLBACK.
 #pragma once
 #include "velo_mlp.cuh"
 
 namespace velo {
 
 constexpr uint32_t kErrorMlpTimeout = 1u;  // queue[6]: the tensor core did not answer in time
+constexpr uint32_t kFillThreads = 256;
+constexpr uint32_t kCandTileBytes = kMlpTile * kMlpK1 * 2;  // 4096
 
 __device__ __forceinline__ uint2 pack_windows(int f0, int l0, int f2, int l2)
 {
@@ -22,19 +33,14 @@ __device__ __forceinline__ uint2 pack_windows(int f0, int l0, int f2, int l2)
                     (static_cast<uint32_t>(f2) & 0xFFFFu) | (static_cast<uint32_t>(l2) << 16));
 }
 
-// Dynamic shared memory of the pruned form: one MlpInferSmem, 128-byte aligned.
-constexpr uint32_t kFillPrunedSmem = sizeof(MlpInferSmem) + 128;
-
 template<bool kPruned>
-__global__ void __launch_bounds__(kMlpTile) fill_candidates_kernel(ChainPointers P)
+__global__ void __launch_bounds__(kFillThreads) fill_candidates_kernel(ChainPointers P)
 {
   __shared__ uint32_t s_ms[kModules + 1];
   __shared__ uint32_t s_event;
-  extern __shared__ uint8_t s_dyn[];
-  MlpInferSmem& sm = *reinterpret_cast<MlpInferSmem*>((reinterpret_cast<uintptr_t>(s_dyn) + 127) & ~uintptr_t(127));
-  uint32_t phase = 0;
-  bool mlp_ok = true;
-  if (kPruned) mlp_infer_setup(sm, P.mlp);
+  __shared__ float s_norm[32];
+  const uint32_t lane = threadIdx.x & 31u;
+  if (kPruned && threadIdx.x < 32) s_norm[threadIdx.x] = P.mlp.norm[threadIdx.x];
 
   for (;;) {
     if (threadIdx.x == 0) s_event = atomicAdd(P.queue + 3, 1u);
@@ -51,16 +57,16 @@ __global__ void __launch_bounds__(kMlpTile) fill_candidates_kernel(ChainPointers
     if (runnable) {
       const float4* H = P.hits.xyzp + base;
       uint2* W = P.windows + base;
-      const bool fallback = kPruned && (nhits > P.mlp.max_hits || !mlp_ok);
+      const bool fallback = kPruned && nhits > P.mlp.max_hits;
       if (kPruned && fallback && threadIdx.x == 0) P.status[e] = status | kStatusMlpFallback;
       const uint32_t lo = s_ms[2], hi = s_ms[50];
       if (kPruned) {
-        // modules 0, 1, 50, 51 hold no h1; their hits stay extension candidates
+        // modules 0, 1, 50, 51 hold no h1: extension candidates only
         uint8_t* K = P.keep + base;
-        for (uint32_t h = threadIdx.x; h < lo; h += kMlpTile) K[h] = 2;
-        for (uint32_t h = hi + threadIdx.x; h < nhits; h += kMlpTile) K[h] = 2;
+        for (uint32_t h = threadIdx.x; h < lo; h += kFillThreads) K[h] = 2;
+        for (uint32_t h = hi + threadIdx.x; h < nhits; h += kFillThreads) K[h] = 2;
       }
-      for (uint32_t t0 = lo; t0 < hi; t0 += kMlpTile) {
+      for (uint32_t t0 = lo; t0 < hi; t0 += kFillThreads) {
         const uint32_t h = t0 + threadIdx.x;
         const bool valid = h < hi;
         int f0 = -1, l0 = -1, f2 = -1, l2 = -1;
@@ -80,27 +86,89 @@ __global__ void __launch_bounds__(kMlpTile) fill_candidates_kernel(ChainPointers
         }
         if (kPruned) {
           const bool cand = valid && f0 != -1 && f2 != -1;
-          uint32_t keep = 3;
-          if (!fallback) {  // uniform over the CTA
+          if (valid) P.keep[base + h] = cand ? 3u : 2u;  // candidates: verdict from score_candidates
+          const bool append = cand && !fallback;
+          // one atomic per warp for the rows of its candidates
+          const uint32_t bal = __ballot_sync(0xFFFFFFFFu, append);
+          uint32_t row0 = 0;
+          if (lane == 0 && bal) row0 = atomicAdd(P.queue + 7, static_cast<uint32_t>(__popc(bal)));
+          row0 = __shfl_sync(0xFFFFFFFFu, row0, 0);
+          if (append) {
+            const uint32_t r = row0 + __popc(bal & ((1u << lane) - 1u));
             float f[kMlpFeatures];
-            if (cand) seed_features(H, P.hit_size + base, h, m, f0, l0, f2, l2, f);
-            mlp_store_features(sm, f, cand);
-            float z0 = 0.f, z1 = 0.f;
-            if (!mlp_tile_forward(sm, phase, z0, z1)) {
-              mlp_ok = false;
-              if (threadIdx.x == 0) atomicOr(P.queue + 6, kErrorMlpTimeout);
-            }
-            if (mlp_ok)
-              keep = cand ? ((z0 >= P.mlp.seed_logit ? 1u : 0u) | ((!P.mlp.use_ext || z1 >= P.mlp.ext_logit) ? 2u : 0u))
-                          : 2u;
+            seed_features(H, P.hit_size + base, h, m, f0, l0, f2, l2, f);
+            store_feature_row(P.cand_feat + static_cast<size_t>(r / kMlpTile) * kCandTileBytes, r % kMlpTile, f,
+                              s_norm);
+            P.cand_slot[r] = base + h;
           }
-          if (valid) P.keep[base + h] = static_cast<uint8_t>(keep);
         }
       }
     }
     __syncthreads();
   }
-  if (kPruned) mlp_infer_teardown(sm);
+}
+
+
+// Shared memory of score_candidates: the inference tile buffers plus two X tiles filled by
+// bulk copies, each with its barrier.
+struct __align__(128) ScoreSmem {
+  MlpInferSmem mlp;
+  uint8_t x[2][kCandTileBytes];
+  uint64_t load_bar[2];
+};
+constexpr uint32_t kScoreSmem = sizeof(ScoreSmem) + 128;
+
+__global__ void __launch_bounds__(kMlpTile) score_candidates_kernel(ChainPointers P)
+{
+  extern __shared__ uint8_t s_dyn[];
+  ScoreSmem& s = *reinterpret_cast<ScoreSmem*>((reinterpret_cast<uintptr_t>(s_dyn) + 127) & ~uintptr_t(127));
+  const uint32_t rows = P.queue[7];
+  const uint32_t tiles = (rows + kMlpTile - 1) / kMlpTile;
+  if (blockIdx.x >= tiles) return;  // uniform: this CTA has no tile
+  if (threadIdx.x == 0) {
+    mbar_init1(&s.load_bar[0]);
+    mbar_init1(&s.load_bar[1]);
+  }
+  mlp_infer_setup(s.mlp, P.mlp);  // includes the barrier that publishes the inits
+  uint32_t mma_phase = 0, load_phase[2] = {0u, 0u};
+  bool ok = true;
+  if (threadIdx.x == 0)
+    bulk_load_smem(s.x[0], P.cand_feat + static_cast<size_t>(blockIdx.x) * kCandTileBytes, kCandTileBytes,
+                   &s.load_bar[0]);
+  uint32_t buf = 0;
+  for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x, buf ^= 1u) {
+    // prefetch the next tile into the other buffer (its previous MMA reads are complete)
+    const uint32_t next = tile + gridDim.x;
+    if (threadIdx.x == 0 && next < tiles)
+      bulk_load_smem(s.x[buf ^ 1u], P.cand_feat + static_cast<size_t>(next) * kCandTileBytes, kCandTileBytes,
+                     &s.load_bar[buf ^ 1u]);
+    const bool loaded = mbar_wait_parity(&s.load_bar[buf], load_phase[buf]);
+    load_phase[buf] ^= 1u;
+    if (!__syncthreads_and(loaded)) {
+      ok = false;
+      break;
+    }
+    float z0 = 0.f, z1 = 0.f;
+    if (!mlp_tile_forward(s.mlp, mma_phase, z0, z1, s.x[buf])) {
+      ok = false;
+      break;
+    }
+    const uint32_t r = tile * kMlpTile + threadIdx.x;
+    if (r < rows) {
+      const uint32_t slot = P.cand_slot[r];
+      const bool seed = z0 >= P.mlp.seed_logit;
+      const bool ext = !P.mlp.use_ext || z1 >= P.mlp.ext_logit;
+      if (!seed) P.windows[slot].x = 0xFFFFu;  // no h0 window: the search skips this h1
+      P.keep[slot] = static_cast<uint8_t>((seed ? 1u : 0u) | (ext ? 2u : 0u));
+    }
+  }
+  if (!ok && threadIdx.x == 0) atomicOr(P.queue + 6, kErrorMlpTimeout);
+  // a bulk copy still in flight (timeout path) must land before the CTA exits
+  if (!ok && threadIdx.x == 0) {
+    mbar_wait_parity(&s.load_bar[0], load_phase[0]);
+    mbar_wait_parity(&s.load_bar[1], load_phase[1]);
+  }
+  mlp_infer_teardown(s.mlp);
 }
 
 }  // namespace velo

@@ -89,6 +89,9 @@ struct ChainPointers {
   // candidates
   uint2* windows;          // [hit capacity] {h0 first | last << 16, h2 first | last << 16}
   uint8_t* keep;           // [hit capacity] learned keep bits; nullptr in the plain mode
+  uint8_t* cand_feat;      // pruned mode: bf16 feature rows of the seeding candidates, 128-row
+                           // tiles of 4 KB in the tensor core's K-major layout
+  uint32_t* cand_slot;     // pruned mode: hit slot of each candidate row
   // search
   SearchScratch scratch;
   uint32_t* event_tracks;      // [N] tracks per event
@@ -104,7 +107,7 @@ struct ChainPointers {
   uint32_t max_track_hits_total;
   uint64_t hit_capacity;       // entries of the hit SoA arrays
   // work queues: [0] decode, [1] warp search, [2] block search, [3] fill_candidates,
-  // [4] / [5] sizes of the warp / block event lists, [6] error bits
+  // [4] / [5] sizes of the warp / block event lists, [6] error bits, [7] candidate rows
   uint32_t* queue;             // [8]
   uint32_t* warp_events;       // [N] events routed to the warp-per-event search
   uint32_t* block_events;      // [N] events routed to the block-per-event search

@@ -152,6 +152,17 @@ __device__ __forceinline__ void load_canon(uint8_t* dst, const __nv_bfloat16* sr
   }
 }
 
+// Bulk copy (no tensor map) of `bytes` from global memory into shared memory, completing
+// on `mbar` with the byte count; 16-byte aligned addresses, size a multiple of 16.
+__device__ __forceinline__ void bulk_load_smem(void* dst, const void* src, uint32_t bytes, uint64_t* mbar)
+{
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mbar)), "r"(bytes) : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                 smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(mbar))
+               : "memory");
+}
+
 // Makes the shared-memory writes of every thread visible to the tensor core and orders
 // earlier tensor-memory reads before the MMAs issued next.
 __device__ __forceinline__ void umma_stage_barrier()
@@ -200,6 +211,7 @@ struct __align__(128) MlpInferSmem {
 constexpr uint32_t kSbo1 = (kMlpK1 / 8) * 128;  // 256
 constexpr uint32_t kSbo2 = (kMlpK2 / 8) * 128;  // 1280
 constexpr uint32_t kMlpInferTmemCols = 64;       // D1, D2 and D3 share columns 0..63
+constexpr uint32_t kMlpInferSmem = sizeof(MlpInferSmem) + 128;  // dynamic size, 128-byte aligned
 
 // Warp 0 allocates tensor memory, thread 0 sets up the barrier; weights to shared memory.
 __device__ __forceinline__ void mlp_infer_setup(MlpInferSmem& s, const MlpDevice& mlp)
@@ -219,6 +231,27 @@ __device__ __forceinline__ void mlp_infer_teardown(MlpInferSmem& s)
   __syncthreads();
   tc_fence_after();
   if (threadIdx.x < 32) tmem_dealloc(s.tmem, kMlpInferTmemCols);
+}
+
+// Row `row` of an X tile at `tile` (shared or global memory): normalised features in
+// bf16 (norm: mean[16], inv_std[16]), 1.0 bias column, zero padding.
+__device__ __forceinline__ void store_feature_row(uint8_t* tile, uint32_t row, const float (&f)[kMlpFeatures],
+                                                  const float* norm)
+{
+  float n[16];
+#pragma unroll
+  for (int i = 0; i < 12; ++i) n[i] = (f[i] - norm[i]) * norm[16 + i];
+  n[12] = 1.f;
+  n[13] = n[14] = n[15] = 0.f;
+#pragma unroll
+  for (uint32_t kb = 0; kb < 2; ++kb) {
+    uint4 v;
+    v.x = pack_bf16x2(n[8 * kb + 0], n[8 * kb + 1]);
+    v.y = pack_bf16x2(n[8 * kb + 2], n[8 * kb + 3]);
+    v.z = pack_bf16x2(n[8 * kb + 4], n[8 * kb + 5]);
+    v.w = pack_bf16x2(n[8 * kb + 6], n[8 * kb + 7]);
+    *reinterpret_cast<uint4*>(tile + canon_off(row, kb, kSbo1)) = v;
+  }
 }
 
 // Writes this thread's row of X: normalised features in bf16, 1.0 bias column.
@@ -275,11 +308,13 @@ __device__ __forceinline__ bool mlp_layer(MlpInferSmem& s, uint32_t& phase, cons
   return umma_wait(&s.mbar, phase);
 }
 
-// Forward pass of the tile staged in s.x; logits of this thread's row. False on timeout.
-__device__ __forceinline__ bool mlp_tile_forward(MlpInferSmem& s, uint32_t& phase, float& z0, float& z1)
+// Forward pass of the X tile at `x` (shared memory, canonical layout; s.x by default);
+// logits of this thread's row. False on timeout.
+__device__ __forceinline__ bool mlp_tile_forward(MlpInferSmem& s, uint32_t& phase, float& z0, float& z1,
+                                                 const uint8_t* x = nullptr)
 {
   const uint32_t taddr_row = s.tmem + ((threadIdx.x & ~31u) << 16);
-  if (!mlp_layer(s, phase, s.x, kSbo1, s.w1, kSbo1, kMlpK1, kMlpHidden)) return false;
+  if (!mlp_layer(s, phase, x ? x : s.x, kSbo1, s.w1, kSbo1, kMlpK1, kMlpHidden)) return false;
   mlp_hidden_epilogue(s.h, taddr_row);
   if (!mlp_layer(s, phase, s.h, kSbo2, s.w2, kSbo2, kMlpK2, kMlpHidden)) return false;
   mlp_hidden_epilogue(s.h, taddr_row);

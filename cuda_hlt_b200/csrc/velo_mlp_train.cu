@@ -30,7 +30,7 @@
 
 #include "../../include/velo_b200.h"
 #include "velo_ctx.hpp"
-#include "velo_fill.cuh"
+#include "velo_mlp.cuh"
 
 using namespace velo;
 
@@ -677,7 +677,7 @@ int velo_mlp_trainer_create(int device, uint64_t max_samples, uint64_t seed, Vel
   ok &= cudaFuncSetAttribute(mlp_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(kTrainSmem)) == cudaSuccess;
   ok &= cudaFuncSetAttribute(mlp_infer_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(kFillPrunedSmem)) == cudaSuccess;
+                             static_cast<int>(kMlpInferSmem)) == cudaSuccess;
   ok &= cudaMemset(t->d_error, 0, 4) == cudaSuccess;
   if (!ok) return fail(VELO_ERR_CUDA);
   // defaults: identity normalisation, seeded uniform(+-1/sqrt(fan_in)) weights, zero biases
@@ -908,7 +908,7 @@ int velo_mlp_infer(VeloMlpTrainer* t, const float* features, uint32_t n, float* 
   m.w = t->d_w;
   m.norm = t->d_norm;
   const uint32_t tiles = (n + kMlpTile - 1) / kMlpTile;
-  mlp_infer_rows_kernel<<<std::min<uint32_t>(tiles, 4 * t->grid), kMlpTile, kFillPrunedSmem, t->stream>>>(
+  mlp_infer_rows_kernel<<<std::min<uint32_t>(tiles, 4 * t->grid), kMlpTile, kMlpInferSmem, t->stream>>>(
     m, d_f, n, d_z, t->d_error);
   const cudaError_t le = cudaGetLastError();
   if (le == cudaSuccess) TCK(cudaMemcpyAsync(logits, d_z, 8ull * n, cudaMemcpyDeviceToHost, t->stream));

@@ -4,8 +4,8 @@
 // (ProcessModules.cu:8-163, TrackForwarding.cu:41-181, TrackSeeding.cu:7-200,
 // WeakTracksAdder.cu:88-115). What changes is the mapping onto the warp:
 //   * seeding: the phi windows of every h1 come precomputed from fill_candidates (in the
-//     pruned mode only h1 with the learned seed-keep bit are considered, and forwarding
-//     skips candidates without the extension-keep bit when that pruning is on);
+//     pruned mode the scorer has cleared the windows of pruned seeds, and forwarding skips
+//     candidates without the extension-keep bit when that pruning is on);
 //     the h1 candidates of a step are compacted into a shared list, their
 //     (h1, h0) pairs are flattened over the lanes, and each h1 keeps its best triplet in a
 //     shared 64-bit key (scatter bits, h0 offset, h2 offset) reduced with atomicMin. The
@@ -190,7 +190,6 @@ __global__ void __launch_bounds__(WPB * 32) search_kernel(ChainPointers P)
       __syncwarp();
       const float4* H = P.hits.xyzp + base;
       const uint2* Wn = P.windows + base;
-      const uint8_t* K = P.keep ? P.keep + base : nullptr;
       const uint8_t* KE = (P.keep && P.mlp.use_ext) ? P.keep + base : nullptr;  // extension pruning
       uint16_t* track_n = P.scratch.track_n + static_cast<size_t>(e) * kMaxTracks;
       uint16_t* track_hits = P.scratch.track_hits + static_cast<size_t>(e) * kMaxTracks * kMaxTrackSize;
@@ -208,21 +207,27 @@ __global__ void __launch_bounds__(WPB * 32) search_kernel(ChainPointers P)
           const uint32_t start = mstart[m], num = mnum[m];
           for (uint32_t r0 = 0; r0 < num; r0 += kSeedChunk) {
             const uint32_t r_end = min(num, r0 + kSeedChunk);
-            // (a) unused h1 with both phi windows (FillCandidates.cu:31-68, TrackSeeding.cu:24-49)
+            // (a) unused h1 with both phi windows (FillCandidates.cu:31-68, TrackSeeding.cu:24-49);
+            // the windows of the chunk's (up to) four 32-hit groups are loaded together so that
+            // their latencies overlap
             uint32_t nc = 0;
-            for (uint32_t r1 = r0; r1 < r_end; r1 += 32) {
-              const uint32_t r = r1 + lane;
+            uint2 wv[kSeedChunk / 32];
+#pragma unroll
+            for (uint32_t j = 0; j < kSeedChunk / 32; ++j) {
+              const uint32_t r = r0 + 32 * j + lane;
+              wv[j] = make_uint2(0xFFFFu, 0xFFFFu);
+              if (r < r_end && !test_used(used, start + r)) wv[j] = Wn[start + r];
+            }
+#pragma unroll
+            for (uint32_t j = 0; j < kSeedChunk / 32; ++j) {
+              const uint32_t r = r0 + 32 * j + lane;
               const uint32_t h1 = start + r;
-              int f0 = -1, l0 = -1, f2 = -1, l2 = -1;
-              bool has = false;
-              if (r < r_end && !test_used(used, h1) && (!K || (K[h1] & 1u))) {
-                const uint2 w = Wn[h1];
-                f0 = static_cast<int>(w.x & 0xFFFFu);
-                l0 = static_cast<int>(w.x >> 16);
-                f2 = static_cast<int>(w.y & 0xFFFFu);
-                l2 = static_cast<int>(w.y >> 16);
-                has = f0 != 0xFFFF && f2 != 0xFFFF;
-              }
+              const uint2 w = wv[j];
+              const int f0 = static_cast<int>(w.x & 0xFFFFu);
+              const int l0 = static_cast<int>(w.x >> 16);
+              const int f2 = static_cast<int>(w.y & 0xFFFFu);
+              const int l2 = static_cast<int>(w.y >> 16);
+              const bool has = r < r_end && f0 != 0xFFFF && f2 != 0xFFFF;
               uint32_t cnt;
               const uint32_t rank = ballot_rank(has, cnt);
               if (has) {

@@ -187,7 +187,6 @@ __global__ void __launch_bounds__(kBlockThreads) search_block_kernel(ChainPointe
       }
       const float4* H = staged ? stage : P.hits.xyzp + base;
       const uint2* Wn = P.windows + base;  // phi windows of every h1 (fill_candidates)
-      const uint8_t* K = P.keep ? P.keep + base : nullptr;
       const uint8_t* KE = (P.keep && P.mlp.use_ext) ? P.keep + base : nullptr;
       uint16_t* track_n = P.scratch.track_n + static_cast<size_t>(ev) * kMaxTracks;
       uint16_t* track_hits = P.scratch.track_hits + static_cast<size_t>(ev) * kMaxTracks * kMaxTrackSize;
@@ -211,7 +210,7 @@ __global__ void __launch_bounds__(kBlockThreads) search_block_kernel(ChainPointe
           if (r < total_h1) {
             const uint32_t m = r < na ? ma : mb;
             h1 = mstart[m] + (r < na ? r : r - na);
-            if (!test_used(used, h1) && (!K || (K[h1] & 1u))) {
+            if (!test_used(used, h1)) {
               const uint2 w = Wn[h1];
               f0 = static_cast<int>(w.x & 0xFFFFu);
               l0 = static_cast<int>(w.x >> 16);
