@@ -201,8 +201,8 @@ def test_trained_scorer_prunes_at_no_efficiency_cost():
     w.max_event_clusters = 0xFFFFFFFF
     t.close()
     ev = events.generate(seed=8, nu_min=2.0, nu_max=15.0, n_events=1024, with_mc=True)
-    plain, st_plain = run_mode(ev, chain.MODE_PLAIN, timing=True)
-    pruned, st_pruned = run_mode(ev, chain.MODE_PRUNED, w, timing=True)
+    plain = run_mode(ev, chain.MODE_PLAIN)
+    pruned = run_mode(ev, chain.MODE_PRUNED, w)
     cp, cq = chain.check_tracks(ev, plain), chain.check_tracks(ev, pruned)
     assert cq.long_efficiency >= cp.long_efficiency - 0.002
     assert cq.ghost_rate <= cp.ghost_rate + 1e-4
@@ -210,4 +210,9 @@ def test_trained_scorer_prunes_at_no_efficiency_cost():
     ms, mn = pruned["module_start"].reshape(-1, 52), pruned["module_num"].reshape(-1, 52)
     keep = np.concatenate([pruned["cluster_keep"][ms[e, 2]:ms[e, 49] + mn[e, 49]] for e in range(ev.n_events)])
     assert (keep & 1).mean() < 0.6
-    assert st_pruned["search_by_triplet"] < st_plain["search_by_triplet"]
+    # the search explores fewer combinations: faster on a full 16,384-event batch (at 1,024
+    # events the search time is the latency of the slowest events, not the work)
+    big = events.generate(seed=8, nu_min=2.0, nu_max=15.0, n_events=16384, first_event=2000, with_mc=False)
+    _, st_plain = run_mode(big, chain.MODE_PLAIN, timing=True)
+    _, st_pruned = run_mode(big, chain.MODE_PRUNED, w, timing=True)
+    assert st_pruned["search_by_triplet"] < 0.95 * st_plain["search_by_triplet"]
