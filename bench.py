@@ -184,12 +184,17 @@ def load_scorer(args):
                "max_event_clusters": max_clusters}
 
 
-def time_form(vc, batch_ptrs, stream, args, world, dist, torch, local_rank):
-    """Warm-up, then K timed steps of one form: (elapsed ms, max over ranks; stage times;
-    clocks during the timed region)."""
+def time_form(vcs, streams, batch_ptrs, args, world, dist, torch, local_rank):
+    """Warm-up, then K timed steps of one form: (elapsed ms, max over ranks; stage times of
+    each context; clocks during the timed region). Batches alternate between the contexts,
+    each on its own stream, so that one batch's kernels fill the SMs that the other's leave
+    idle (kernel tails, latency-bound phases)."""
+    cur = torch.cuda.current_stream()
+
     def step():
-        for raw_p, off_p, n in batch_ptrs:
-            vc.run_device(raw_p, off_p, n, stream)
+        for k, (raw_p, off_p, n) in enumerate(batch_ptrs):
+            j = k % len(vcs)
+            vcs[j].run_device(raw_p, off_p, n, streams[j].cuda_stream)
 
     for _ in range(args.warmup):
         step()
@@ -197,14 +202,19 @@ def time_form(vc, batch_ptrs, stream, args, world, dist, torch, local_rank):
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    vc.set_timing(True)  # keep only the timed region's event records
+    for vc in vcs:
+        vc.set_timing(True)  # keep only the timed region's event records
     start = torch.cuda.Event(enable_timing=True)
     end = torch.cuda.Event(enable_timing=True)
     with ClockSampler(local_rank) as clocks:
-        start.record()
+        start.record(cur)
+        for s in streams:
+            s.wait_event(start)
         for _ in range(args.steps):
             step()
-        end.record()
+        for s in streams:
+            cur.wait_stream(s)
+        end.record(cur)
         torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -213,7 +223,11 @@ def time_form(vc, batch_ptrs, stream, args, world, dist, torch, local_rank):
         t = torch.tensor([elapsed_ms], device=torch.device("cuda", local_rank))
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         elapsed_ms = float(t.item())
-    return elapsed_ms, vc.stage_times(), clocks.summary()
+    stages = {}
+    for vc in vcs:
+        for k, v in vc.stage_times().items():
+            stages[k] = stages.get(k, 0) + v
+    return elapsed_ms, stages, clocks.summary()
 
 
 def roofline(stages, census, n_events, n_batches, peak, peak_kind, traffic_table):
@@ -303,13 +317,18 @@ def run_ours(args, rank, world, local_rank):
     from cuda_hlt_b200 import autotune
 
     forms = {}
+    streams = [torch.cuda.Stream(device=dev) for _ in range(args.streams)]
     for name, mode in (("plain", chain.MODE_PLAIN), ("pruned", chain.MODE_PRUNED)):
-        vc = chain.VeloChain(max_events=BUCKET, max_raw_bytes=max_batch_bytes + 4096, device=local_rank,
-                             use_graphs=True)
-        vc.set_mlp(weights)
-        vc.set_mode(mode)
+        vcs = [chain.VeloChain(max_events=BUCKET, max_raw_bytes=max_batch_bytes + 4096, device=local_rank,
+                               use_graphs=True) for _ in range(args.streams)]
+        for vc in vcs:
+            vc.set_mlp(weights)
+            vc.set_mode(mode)
+        vc = vcs[0]
         # search mapping per hit-count bucket, tuned on the first batch (outside the timed region)
         threshold, tune_ms = autotune.tune_block_threshold(vc, *batch_ptrs[0], stream)
+        for other in vcs[1:]:
+            other.set_block_threshold(threshold)
         # census: per-batch totals for the algorithmic-byte accounting and the fallback share
         census = dict(clusters=0, tracks=0, track_hits=0, raw_bytes=raw_bytes, fallback_events=0)
         for raw_p, off_p, n in batch_ptrs:
@@ -323,7 +342,7 @@ def run_ours(args, rank, world, local_rank):
                          "velo_download")
             census["fallback_events"] += int(((st & chain.STATUS["mlp_fallback"]) != 0).sum())
         launches = vc.launch_count()
-        elapsed_ms, stages, clocks = time_form(vc, batch_ptrs, stream, args, world, dist, torch, local_rank)
+        elapsed_ms, stages, clocks = time_form(vcs, streams, batch_ptrs, args, world, dist, torch, local_rank)
         roof, stage_ms = roofline(stages, census, n_events, n_batches, peak, peak_kind, traffic_table)
         forms[name] = {"value": n_events * world * args.steps / (elapsed_ms / 1e3),
                        "ms_per_step": elapsed_ms / args.steps,
@@ -332,7 +351,8 @@ def run_ours(args, rank, world, local_rank):
                        "search_mapping": {"block_above_clusters": threshold,
                                           "search_ms_per_threshold": {str(k): v for k, v in tune_ms.items()}},
                        "gpu_launches": launches * n_batches * args.steps, "clocks": clocks, "threshold": threshold}
-        vc.close()
+        for v in vcs:
+            v.close()
         log(f"[rank {rank}] {name}: {forms[name]['value']:.0f} events/s")
 
     # ---- track quality of both forms on the MC-carrying head of the workload ----
@@ -350,6 +370,7 @@ def run_ours(args, rank, world, local_rank):
                                f"rank*{n_events}..., MLP-pruned search; events above the scorer's trained "
                                f"occupancy fall back to the plain search", "events_per_gpu": n_events,
                    "batch_events": BUCKET, "batches_per_step": n_batches, "mode": "pruned", "graphs": True,
+                   "streams": args.streams,
                    "scorer": scorer_info, "search_mapping": p["search_mapping"],
                    "l2": f"inputs larger than L2 ({raw_bytes / 1e9:.2f} GB raw banks per step)",
                    "parallelism": f"event shards x{world}"},
@@ -541,6 +562,7 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=16384)
     ap.add_argument("--reference-sample", type=int, default=8192)
     ap.add_argument("--quality-events", type=int, default=32768, help="MC-checked events of the workload head")
+    ap.add_argument("--streams", type=int, default=2, help="contexts / streams that batches alternate between")
     ap.add_argument("--weights", default=None, help="scorer weights (default: the committed file)")
     ap.add_argument("--retrain", action="store_true", help="train the scorer here instead of loading it")
     ap.add_argument("--no-extras", action="store_true", help="skip the CPU baseline and reference-GPU legs")

@@ -357,11 +357,14 @@ int velo_create(const VeloConfig* cfg, const void* geometry, size_t geometry_byt
   c->fill_blocks = static_cast<uint32_t>(std::max(1, occ) * c->sm_count);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fill_candidates_kernel<true>, kFillThreads, 0);
   c->fill_pruned_blocks = static_cast<uint32_t>(std::max(1, occ) * c->sm_count);
-  // the scorer holds 64 tensor-memory columns per CTA: at most 8 CTAs per SM
+  // the scorer: as many CTAs per SM as shared memory holds (1 KB of it is reserved per
+  // block), at most 8 (each holds 64 of the SM's 512 tensor-memory columns)
   cudaFuncSetAttribute(score_candidates_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        static_cast<int>(kScoreSmem));
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, score_candidates_kernel, kMlpTile, kScoreSmem);
-  c->score_blocks = static_cast<uint32_t>(std::min(std::max(1, occ), 8) * c->sm_count);
+  int smem_sm = 0;
+  cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c->device);
+  const int score_per_sm = std::max(1, std::min(8, smem_sm / static_cast<int>(kScoreSmem + 1024)));
+  c->score_blocks = static_cast<uint32_t>(score_per_sm * c->sm_count);
   c->mode = cfg->mode == VELO_MODE_PRUNED ? VELO_MODE_PRUNED : VELO_MODE_PLAIN;
   // mapping: VELO_MAP_WARP keeps every event on warps, VELO_MAP_BLOCK on blocks; the
   // default splits at a cluster count (velo_set_block_threshold / the autotuner move it)

@@ -109,11 +109,11 @@ __global__ void __launch_bounds__(kFillThreads) fill_candidates_kernel(ChainPoin
 }
 
 
-// Shared memory of score_candidates: the inference tile buffers plus two X tiles filled by
-// bulk copies, each with its barrier.
+// Shared memory of score_candidates: the inference tile buffers (whose X tile is the first
+// of the two bulk-copy buffers) plus the second X tile, each with its barrier.
 struct __align__(128) ScoreSmem {
   MlpInferSmem mlp;
-  uint8_t x[2][kCandTileBytes];
+  uint8_t x1[kCandTileBytes];
   uint64_t load_bar[2];
 };
 constexpr uint32_t kScoreSmem = sizeof(ScoreSmem) + 128;
@@ -132,15 +132,16 @@ __global__ void __launch_bounds__(kMlpTile) score_candidates_kernel(ChainPointer
   mlp_infer_setup(s.mlp, P.mlp);  // includes the barrier that publishes the inits
   uint32_t mma_phase = 0, load_phase[2] = {0u, 0u};
   bool ok = true;
+  uint8_t* const xbuf[2] = {s.mlp.x, s.x1};
   if (threadIdx.x == 0)
-    bulk_load_smem(s.x[0], P.cand_feat + static_cast<size_t>(blockIdx.x) * kCandTileBytes, kCandTileBytes,
+    bulk_load_smem(xbuf[0], P.cand_feat + static_cast<size_t>(blockIdx.x) * kCandTileBytes, kCandTileBytes,
                    &s.load_bar[0]);
   uint32_t buf = 0;
   for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x, buf ^= 1u) {
     // prefetch the next tile into the other buffer (its previous MMA reads are complete)
     const uint32_t next = tile + gridDim.x;
     if (threadIdx.x == 0 && next < tiles)
-      bulk_load_smem(s.x[buf ^ 1u], P.cand_feat + static_cast<size_t>(next) * kCandTileBytes, kCandTileBytes,
+      bulk_load_smem(xbuf[buf ^ 1u], P.cand_feat + static_cast<size_t>(next) * kCandTileBytes, kCandTileBytes,
                      &s.load_bar[buf ^ 1u]);
     const bool loaded = mbar_wait_parity(&s.load_bar[buf], load_phase[buf]);
     load_phase[buf] ^= 1u;
@@ -149,7 +150,7 @@ __global__ void __launch_bounds__(kMlpTile) score_candidates_kernel(ChainPointer
       break;
     }
     float z0 = 0.f, z1 = 0.f;
-    if (!mlp_tile_forward(s.mlp, mma_phase, z0, z1, s.x[buf])) {
+    if (!mlp_tile_forward(s.mlp, mma_phase, z0, z1, xbuf[buf])) {
       ok = false;
       break;
     }

@@ -149,12 +149,50 @@ struct SeedSlots {
   unsigned long long last[kSeedChunk];
 };
 
+// Forwarding reads the phi of its two target modules from shared memory; the staging
+// area reuses the seeding slots (the two phases never overlap).
+constexpr uint32_t kFwdStage = sizeof(SeedSlots) / (2 * sizeof(float));
+
 struct SearchWarpShared {
   uint32_t used[kEventHitCap / 32];
   uint32_t mstart[kModules];
   uint32_t mnum[kModules];
-  SeedSlots seed;
+  union {
+    SeedSlots seed;
+    float fphi[2][kFwdStage];
+  } u;
 };
+
+// phi window of a forwarded track in one module (TrackForwarding.cuh:28-59), with the
+// module's phi staged in shared memory (`sphi`, null when the module did not fit): the
+// same probes on the same values as phi_window4 over the cluster records.
+__device__ __forceinline__ void forward_window_staged(const float4* H, const float* sphi, uint32_t mstart,
+                                                      uint32_t mnum, float mz, float tx, float ty, float h0x,
+                                                      float h0y, float h0z, bool odd, int& first, int& last,
+                                                      uint32_t& flags)
+{
+  if (!sphi) {
+    forward_window(H, mstart, mnum, mz, tx, ty, h0x, h0y, h0z, odd, first, last, flags);
+    return;
+  }
+  const float dz = mz - h0z;
+  const float predx = tx * dz;
+  const float predy = ty * dz;
+  const float x_prediction = h0x + predx;
+  const float y_prediction = h0y + predy;
+  const float phi = odd ? phi_odd_side(x_prediction, y_prediction) : phi_even_side(x_prediction, y_prediction);
+  first = -1;
+  last = -1;
+  if (mnum == 0) {
+    flags |= kStatusEmptyModuleRead;
+    return;
+  }
+  phi_window(sphi, 0, mnum, phi, kForwardPhiTolerance, first, last);
+  if (first != -1) {
+    first += static_cast<int>(mstart);
+    last += static_cast<int>(mstart);
+  }
+}
 
 template<int WPB>
 __global__ void __launch_bounds__(WPB * 32) search_kernel(ChainPointers P)
@@ -165,7 +203,7 @@ __global__ void __launch_bounds__(WPB * 32) search_kernel(ChainPointers P)
   uint32_t* used = sw.used;
   uint32_t* mstart = sw.mstart;
   uint32_t* mnum = sw.mnum;
-  SeedSlots& sl = sw.seed;
+  SeedSlots& sl = sw.u.seed;
 
   for (;;) {
     uint32_t q = 0;
@@ -328,6 +366,17 @@ __global__ void __launch_bounds__(WPB * 32) search_kernel(ChainPointers P)
         const uint32_t mo = first - 4, me = first - 5;
         const uint32_t mos = mstart[mo], mon = mnum[mo], mes = mstart[me], men = mnum[me];
         const float moz = c_module_z[mo], mez = c_module_z[me];
+        // stage the phi of both target modules (their binary searches then stay in shared
+        // memory); a module above the staging size is searched in global memory
+        const float* sphi_o = mon <= kFwdStage ? sw.u.fphi[0] : nullptr;
+        const float* sphi_e = men <= kFwdStage ? sw.u.fphi[1] : nullptr;
+        if (diff > 0) {
+          if (sphi_o)
+            for (uint32_t i = lane; i < mon; i += 32) sw.u.fphi[0][i] = H[mos + i].w;
+          if (sphi_e)
+            for (uint32_t i = lane; i < men; i += 32) sw.u.fphi[1][i] = H[mes + i].w;
+        }
+        __syncwarp();
         for (uint32_t i0 = 0; i0 < diff; i0 += 32) {
           const uint32_t i = i0 + lane;
           int action = 0;  // 1 extend, 2 keep with a skipped module, 3 demote to weak
@@ -360,8 +409,8 @@ __global__ void __launch_bounds__(WPB * 32) search_kernel(ChainPointers P)
             const float ty = tyn * td;
             float best_fit = 3.402823466e+38f;
             int of, ol, ef, el;
-            forward_window(H, mos, mon, moz, tx, ty, h0.x, h0.y, h0.z, true, of, ol, flags);
-            forward_window(H, mes, men, mez, tx, ty, h0.x, h0.y, h0.z, false, ef, el, flags);
+            forward_window_staged(H, sphi_o, mos, mon, moz, tx, ty, h0.x, h0.y, h0.z, true, of, ol, flags);
+            forward_window_staged(H, sphi_e, mes, men, mez, tx, ty, h0.x, h0.y, h0.z, false, ef, el, flags);
             const int n_odd = ol - of, n_even = el - ef;
             for (int j = 0; j < n_odd + n_even; ++j) {
               const int h2i = j < n_odd ? of + j : ef + j - n_odd;

@@ -60,7 +60,7 @@ __global__ void __launch_bounds__(128) search_static_kernel(StaticSearchArgs A)
   uint32_t* used = sw.used;
   uint32_t* mstart = sw.mstart;
   uint32_t* mnum = sw.mnum;
-  SeedSlots& sl = sw.seed;
+  SeedSlots& sl = sw.u.seed;
   uint32_t* queue = reinterpret_cast<uint32_t*>(A.scratch);
 
   for (;;) {
