@@ -109,53 +109,14 @@ __global__ void __launch_bounds__(kFillThreads) fill_candidates_kernel(ChainPoin
 }
 
 
-// score_candidates processes kScoreTiles tiles per iteration with the same 128 threads
-// (thread t owns row t of each): the MMAs of all of them go out under one barrier and one
-// commit, so the fixed cost of a layer (barriers, commit round trip, tensor-memory loads)
-// is shared. Accumulators of tile i sit in tensor-memory columns [64 i, 64 i + 64).
-constexpr uint32_t kScoreTiles = 2;
-constexpr uint32_t kScoreTmemCols = 64 * kScoreTiles;
-
+// Shared memory of score_candidates: the inference tile buffers (whose X tile is the first
+// of the two bulk-copy buffers) plus the second X tile, each with its barrier.
 struct __align__(128) ScoreSmem {
-  uint8_t w1[kMlpW1 * 2];
-  uint8_t w2[kMlpW2 * 2];
-  uint8_t w3[kMlpW3 * 2];
-  uint8_t h[kScoreTiles][kMlpTile * kMlpK2 * 2];
-  uint8_t x[2][kScoreTiles][kCandTileBytes];  // double-buffered X tiles
-  uint64_t mma_bar;
+  MlpInferSmem mlp;
+  uint8_t x1[kCandTileBytes];
   uint64_t load_bar[2];
-  uint32_t tmem;
 };
 constexpr uint32_t kScoreSmem = sizeof(ScoreSmem) + 128;
-
-// Issues the copies of the X tiles of group g (tiles g*kScoreTiles ...) into buffer `buf`.
-__device__ __forceinline__ void score_load_group(ScoreSmem& s, const ChainPointers& P, uint32_t g, uint32_t tiles,
-                                                 uint32_t buf)
-{
-  const uint32_t t0 = g * kScoreTiles;
-  const uint32_t n = min(kScoreTiles, tiles - t0);
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(&s.load_bar[buf])),
-               "r"(n * kCandTileBytes)
-               : "memory");
-  for (uint32_t i = 0; i < n; ++i)
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   smem_u32(s.x[buf][i])),
-                 "l"(P.cand_feat + static_cast<size_t>(t0 + i) * kCandTileBytes), "r"(kCandTileBytes),
-                 "r"(smem_u32(&s.load_bar[buf]))
-                 : "memory");
-}
-
-// One layer for all tiles of the group: D_i = A_i * B^T into columns 64 i, then wait.
-__device__ __forceinline__ bool score_layer(ScoreSmem& s, uint32_t& phase, const uint8_t* const* a, uint32_t a_sbo,
-                                            const uint8_t* b, uint32_t b_sbo, uint32_t k, uint32_t n)
-{
-  umma_stage_barrier();
-  if (threadIdx.x == 0) {
-    for (uint32_t i = 0; i < kScoreTiles; ++i) umma_issue(s.tmem + 64 * i, a[i], a_sbo, b, b_sbo, k, n, false);
-    umma_commit(&s.mma_bar);
-  }
-  return umma_wait(&s.mma_bar, phase);
-}
 
 __global__ void __launch_bounds__(kMlpTile) score_candidates_kernel(ChainPointers P)
 {
@@ -163,61 +124,52 @@ __global__ void __launch_bounds__(kMlpTile) score_candidates_kernel(ChainPointer
   ScoreSmem& s = *reinterpret_cast<ScoreSmem*>((reinterpret_cast<uintptr_t>(s_dyn) + 127) & ~uintptr_t(127));
   const uint32_t rows = P.queue[7];
   const uint32_t tiles = (rows + kMlpTile - 1) / kMlpTile;
-  const uint32_t groups = (tiles + kScoreTiles - 1) / kScoreTiles;
-  if (blockIdx.x >= groups) return;  // uniform: this CTA has no work
-  if (threadIdx.x < 32) tmem_alloc(&s.tmem, kScoreTmemCols);
+  if (blockIdx.x >= tiles) return;  // uniform: this CTA has no tile
   if (threadIdx.x == 0) {
-    mbar_init1(&s.mma_bar);
     mbar_init1(&s.load_bar[0]);
     mbar_init1(&s.load_bar[1]);
   }
-  load_canon(s.w1, P.mlp.w, kMlpHidden, kMlpK1);
-  load_canon(s.w2, P.mlp.w + kMlpW1, kMlpHidden, kMlpK2);
-  load_canon(s.w3, P.mlp.w + kMlpW1 + kMlpW2, kMlpOutPad, kMlpK2);
-  umma_stage_barrier();
-  if (threadIdx.x == 0) score_load_group(s, P, blockIdx.x, tiles, 0);
-  const uint32_t lane_addr = s.tmem + ((threadIdx.x & ~31u) << 16);
-  const uint8_t* const hp[kScoreTiles] = {s.h[0], s.h[1]};
-  uint32_t mma_phase = 0, load_phase[2] = {0u, 0u}, buf = 0;
+  mlp_infer_setup(s.mlp, P.mlp);  // includes the barrier that publishes the inits
+  uint32_t mma_phase = 0, load_phase[2] = {0u, 0u};
   bool ok = true;
-  for (uint32_t g = blockIdx.x; g < groups; g += gridDim.x, buf ^= 1u) {
-    // prefetch the next group into the other buffer (its MMAs are complete)
-    if (threadIdx.x == 0 && g + gridDim.x < groups) score_load_group(s, P, g + gridDim.x, tiles, buf ^ 1u);
+  uint8_t* const xbuf[2] = {s.mlp.x, s.x1};
+  if (threadIdx.x == 0)
+    bulk_load_smem(xbuf[0], P.cand_feat + static_cast<size_t>(blockIdx.x) * kCandTileBytes, kCandTileBytes,
+                   &s.load_bar[0]);
+  uint32_t buf = 0;
+  for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x, buf ^= 1u) {
+    // prefetch the next tile into the other buffer (its previous MMA reads are complete)
+    const uint32_t next = tile + gridDim.x;
+    if (threadIdx.x == 0 && next < tiles)
+      bulk_load_smem(xbuf[buf ^ 1u], P.cand_feat + static_cast<size_t>(next) * kCandTileBytes, kCandTileBytes,
+                     &s.load_bar[buf ^ 1u]);
     const bool loaded = mbar_wait_parity(&s.load_bar[buf], load_phase[buf]);
     load_phase[buf] ^= 1u;
     if (!__syncthreads_and(loaded)) {
       ok = false;
       break;
     }
-    const uint8_t* const xp[kScoreTiles] = {s.x[buf][0], s.x[buf][1]};
-    if (!(ok = score_layer(s, mma_phase, xp, kSbo1, s.w1, kSbo1, kMlpK1, kMlpHidden))) break;
-    for (uint32_t i = 0; i < kScoreTiles; ++i) mlp_hidden_epilogue(s.h[i], lane_addr + 64 * i);
-    if (!(ok = score_layer(s, mma_phase, hp, kSbo2, s.w2, kSbo2, kMlpK2, kMlpHidden))) break;
-    for (uint32_t i = 0; i < kScoreTiles; ++i) mlp_hidden_epilogue(s.h[i], lane_addr + 64 * i);
-    if (!(ok = score_layer(s, mma_phase, hp, kSbo2, s.w3, kSbo2, kMlpK2, kMlpOutPad))) break;
-    for (uint32_t i = 0; i < kScoreTiles; ++i) {
-      float v[16];
-      tmem_ld16(lane_addr + 64 * i, v);
-      tmem_ld_wait();
-      const uint32_t r = (g * kScoreTiles + i) * kMlpTile + threadIdx.x;
-      if (r < rows) {
-        const uint32_t slot = P.cand_slot[r];
-        const bool seed = v[0] >= P.mlp.seed_logit;
-        const bool ext = !P.mlp.use_ext || v[1] >= P.mlp.ext_logit;
-        if (!seed) P.windows[slot].x = 0xFFFFu;  // no h0 window: the search skips this h1
-        P.keep[slot] = static_cast<uint8_t>((seed ? 1u : 0u) | (ext ? 2u : 0u));
-      }
+    float z0 = 0.f, z1 = 0.f;
+    if (!mlp_tile_forward(s.mlp, mma_phase, z0, z1, xbuf[buf])) {
+      ok = false;
+      break;
+    }
+    const uint32_t r = tile * kMlpTile + threadIdx.x;
+    if (r < rows) {
+      const uint32_t slot = P.cand_slot[r];
+      const bool seed = z0 >= P.mlp.seed_logit;
+      const bool ext = !P.mlp.use_ext || z1 >= P.mlp.ext_logit;
+      if (!seed) P.windows[slot].x = 0xFFFFu;  // no h0 window: the search skips this h1
+      P.keep[slot] = static_cast<uint8_t>((seed ? 1u : 0u) | (ext ? 2u : 0u));
     }
   }
+  if (!ok && threadIdx.x == 0) atomicOr(P.queue + 6, kErrorMlpTimeout);
+  // a bulk copy still in flight (timeout path) must land before the CTA exits
   if (!ok && threadIdx.x == 0) {
-    atomicOr(P.queue + 6, kErrorMlpTimeout);
-    // a bulk copy still in flight must land before the CTA exits
-    mbar_wait_parity(&s.load_bar[buf ^ 1u], load_phase[buf ^ 1u]);
+    mbar_wait_parity(&s.load_bar[0], load_phase[0]);
+    mbar_wait_parity(&s.load_bar[1], load_phase[1]);
   }
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
-  if (threadIdx.x < 32) tmem_dealloc(s.tmem, kScoreTmemCols);
+  mlp_infer_teardown(s.mlp);
 }
 
 }  // namespace velo
