@@ -158,6 +158,7 @@ __device__ __forceinline__ bool flood_window(uint32_t px0, uint32_t px1, uint32_
 }
 
 constexpr uint32_t kCandCap = 4096;    // candidate pixels listed per event (more: flooded inline)
+constexpr uint32_t kBankMapCap = 16384; // SPs per event with a bank map (more: binary search)
 constexpr uint32_t kRegSortMax = 128;  // modules up to this size are sorted in registers
 
 struct DecodeShared {
@@ -189,7 +190,13 @@ struct DecodeEvent {
   uint32_t stage_base;      // first staging slot of the event
   float4* stage;
   uint32_t* stage_id;
+  const uint8_t* bank_map;  // bank of each flat SP index (shared memory), or null
 };
+
+__device__ __forceinline__ uint32_t bank_of_sp(const DecodeShared& sh, const DecodeEvent& d, uint32_t f)
+{
+  return d.bank_map ? d.bank_map[f] : bank_of(sh, f);
+}
 
 // Bits 26-27 of an LHCb VP id are always zero (sensor < 208 ends at bit 25): the staging
 // record carries the cluster's pixel count there, at most 3.
@@ -213,7 +220,7 @@ __device__ __forceinline__ void stage_cluster(DecodeShared& sh, const DecodeEven
 __device__ __forceinline__ void flood_candidate(DecodeShared& sh, const DecodeEvent& d, const GeometryView& g,
                                                 uint32_t f, uint32_t k)
 {
-  const uint32_t b = bank_of(sh, f);
+  const uint32_t b = bank_of_sp(sh, d, f);
   const uint32_t s = f - sh.sp_prefix[b];
   const uint32_t* bank = d.ev + sh.bank_start[b];
   const uint32_t count = sh.bank_count[b];
@@ -241,27 +248,29 @@ __device__ __forceinline__ unsigned long long cluster_key(const float4* src, con
          (static_cast<unsigned long long>(src_id[i] & 0xFFFFFu) << 12) | i;
 }
 
+// Compare-exchange of elements a (lower index) and b in bitonic order `up`.
+__device__ __forceinline__ void bitonic_cx(unsigned long long& a, unsigned long long& b, bool up)
+{
+  const unsigned long long lo = min(a, b), hi = max(a, b);
+  a = up ? lo : hi;
+  b = up ? hi : lo;
+}
+
 // Bitonic sort of 32 * 4 keys held 4 per lane (element j * 32 + lane), first `size`
-// elements (a power of two, 32..128).
+// elements (a power of two, 32..128). Every register index is a compile-time constant, so
+// the keys stay in registers.
 __device__ __forceinline__ void warp_register_sort(unsigned long long (&key)[4], uint32_t size)
 {
   const uint32_t lane = lane_id();
   const uint32_t per = size >> 5;
   for (uint32_t k = 2; k <= size; k <<= 1) {
     for (uint32_t d = k >> 1; d > 0; d >>= 1) {
-      if (d >= 32) {
-        const uint32_t dj = d >> 5;
-#pragma unroll
-        for (uint32_t j = 0; j < 4; ++j) {
-          if (j >= per || (j & dj)) continue;
-          const uint32_t jj = j | dj;
-          const bool up = ((j * 32 + lane) & k) == 0;
-          const unsigned long long a = key[j], b = key[jj];
-          if ((a > b) == up) {
-            key[j] = b;
-            key[jj] = a;
-          }
-        }
+      if (d == 64) {  // registers j and j + 2 (size 128)
+        bitonic_cx(key[0], key[2], ((0 * 32 + lane) & k) == 0);
+        bitonic_cx(key[1], key[3], ((1 * 32 + lane) & k) == 0);
+      } else if (d == 32) {  // registers j and j + 1
+        bitonic_cx(key[0], key[1], ((0 * 32 + lane) & k) == 0);
+        if (per == 4) bitonic_cx(key[2], key[3], ((2 * 32 + lane) & k) == 0);
       } else {
 #pragma unroll
         for (uint32_t j = 0; j < 4; ++j) {
@@ -303,7 +312,10 @@ __global__ void __launch_bounds__(W * 32) decode_cluster_sort_kernel(ChainPointe
   __shared__ DecodeShared sh;
   // the candidate list and the per-warp sort buffers are never live together
   __shared__ union {
-    uint32_t cand[kCandCap];
+    struct {
+      uint32_t cand[kCandCap];
+      uint8_t bank_map[kBankMapCap];  // flat SP index -> bank, saves a binary search per SP
+    } lists;
     unsigned long long key[W][kSortCap];
   } su;
   const uint32_t warp = threadIdx.x >> 5, lane = lane_id();
@@ -387,11 +399,17 @@ __global__ void __launch_bounds__(W * 32) decode_cluster_sort_kernel(ChainPointe
     __syncthreads();
     const uint32_t total_sp = sh.sp_prefix[kSensors];
     const uint32_t base = static_cast<uint32_t>(off / 4);
-    const DecodeEvent d{ev, 2 * base, P.stage.xyzp, P.stage.id};
+    const bool use_map = event_ok && total_sp <= kBankMapCap;  // counts are valid only then
+    if (use_map) {
+      for (uint32_t b = warp; b < kSensors; b += W)
+        for (uint32_t i = lane; i < sh.bank_count[b]; i += 32) su.lists.bank_map[sh.sp_prefix[b] + i] = static_cast<uint8_t>(b);
+      __syncthreads();
+    }
+    const DecodeEvent d{ev, 2 * base, P.stage.xyzp, P.stage.id, use_map ? su.lists.bank_map : nullptr};
     // ---- pass 1: isolated SPs, candidate search of the others ----
     uint32_t my_cands = 0;
     for (uint32_t f = threadIdx.x; f < total_sp; f += blockDim.x) {
-      const uint32_t b = bank_of(sh, f);
+      const uint32_t b = bank_of_sp(sh, d, f);
       const uint32_t s = f - sh.sp_prefix[b];
       const uint32_t* bank = ev + sh.bank_start[b];
       const uint32_t word = __ldg(bank + s);
@@ -423,7 +441,7 @@ __global__ void __launch_bounds__(W * 32) decode_cluster_sort_kernel(ChainPointe
         ++my_cands;
         const uint32_t k = candidate_k(nib) + 2 * half;
         const uint32_t slot = atomicAdd(&sh.n_list, 1u);
-        if (slot < kCandCap) su.cand[slot] = (f << 4) | k;
+        if (slot < kCandCap) su.lists.cand[slot] = (f << 4) | k;
         else flood_candidate(sh, d, g, f, k);
       }
     }
@@ -434,7 +452,7 @@ __global__ void __launch_bounds__(W * 32) decode_cluster_sort_kernel(ChainPointe
     // ---- pass 2: flood fill of the listed candidates ----
     const uint32_t n_list = min(sh.n_list, kCandCap);
     for (uint32_t i = threadIdx.x; i < n_list; i += blockDim.x) {
-      const uint32_t c = su.cand[i];
+      const uint32_t c = su.lists.cand[i];
       flood_candidate(sh, d, g, c >> 4, c & 0xFu);
     }
     __syncthreads();
