@@ -109,12 +109,14 @@ __global__ void __launch_bounds__(kFillThreads) fill_candidates_kernel(ChainPoin
 }
 
 
-// Shared memory of score_candidates: the inference tile buffers (whose X tile is the first
-// of the two bulk-copy buffers) plus the second X tile, each with its barrier.
+// Shared memory of score_candidates: the inference tile buffers (whose X tile is slot 0 of
+// the copy ring) plus kScoreRing - 1 more X tiles, each slot with its barrier. Tiles are
+// prefetched kScoreRing - 1 ahead, so every CTA keeps several 4 KB copies in flight.
+constexpr uint32_t kScoreRing = 4;
 struct __align__(128) ScoreSmem {
   MlpInferSmem mlp;
-  uint8_t x1[kCandTileBytes];
-  uint64_t load_bar[2];
+  uint8_t x[kScoreRing - 1][kCandTileBytes];
+  uint64_t load_bar[kScoreRing];
 };
 constexpr uint32_t kScoreSmem = sizeof(ScoreSmem) + 128;
 
@@ -125,49 +127,57 @@ __global__ void __launch_bounds__(kMlpTile) score_candidates_kernel(ChainPointer
   const uint32_t rows = P.queue[7];
   const uint32_t tiles = (rows + kMlpTile - 1) / kMlpTile;
   if (blockIdx.x >= tiles) return;  // uniform: this CTA has no tile
-  if (threadIdx.x == 0) {
-    mbar_init1(&s.load_bar[0]);
-    mbar_init1(&s.load_bar[1]);
-  }
-  mlp_infer_setup(s.mlp, P.mlp);  // includes the barrier that publishes the inits
-  uint32_t mma_phase = 0, load_phase[2] = {0u, 0u};
-  bool ok = true;
-  uint8_t* const xbuf[2] = {s.mlp.x, s.x1};
   if (threadIdx.x == 0)
-    bulk_load_smem(xbuf[0], P.cand_feat + static_cast<size_t>(blockIdx.x) * kCandTileBytes, kCandTileBytes,
-                   &s.load_bar[0]);
-  uint32_t buf = 0;
-  for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x, buf ^= 1u) {
-    // prefetch the next tile into the other buffer (its previous MMA reads are complete)
-    const uint32_t next = tile + gridDim.x;
-    if (threadIdx.x == 0 && next < tiles)
-      bulk_load_smem(xbuf[buf ^ 1u], P.cand_feat + static_cast<size_t>(next) * kCandTileBytes, kCandTileBytes,
-                     &s.load_bar[buf ^ 1u]);
-    const bool loaded = mbar_wait_parity(&s.load_bar[buf], load_phase[buf]);
-    load_phase[buf] ^= 1u;
+    for (uint32_t i = 0; i < kScoreRing; ++i) mbar_init1(&s.load_bar[i]);
+  mlp_infer_setup(s.mlp, P.mlp);  // includes the barrier that publishes the inits
+  uint8_t* xbuf[kScoreRing];
+  xbuf[0] = s.mlp.x;
+  for (uint32_t i = 1; i < kScoreRing; ++i) xbuf[i] = s.x[i - 1];
+  uint32_t mma_phase = 0, load_phase = 0;  // load_phase: bit i = parity of slot i
+  bool ok = true;
+  // this CTA's tiles are blockIdx.x + k * gridDim.x, k = 0, 1, ...; tile k goes to slot k % ring
+  if (threadIdx.x == 0)
+    for (uint32_t k = 0; k + 1 < kScoreRing; ++k) {
+      const uint32_t t = blockIdx.x + k * gridDim.x;
+      if (t < tiles)
+        bulk_load_smem(xbuf[k], P.cand_feat + static_cast<size_t>(t) * kCandTileBytes, kCandTileBytes,
+                       &s.load_bar[k]);
+    }
+  uint32_t k = 0;
+  for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++k) {
+    const uint32_t slot = k % kScoreRing;
+    // refill the slot used by tile k - 1 (its MMAs are complete) with tile k + ring - 1
+    const uint32_t ahead = tile + (kScoreRing - 1) * gridDim.x;
+    if (threadIdx.x == 0 && ahead < tiles) {
+      const uint32_t as = (k + kScoreRing - 1) % kScoreRing;
+      bulk_load_smem(xbuf[as], P.cand_feat + static_cast<size_t>(ahead) * kCandTileBytes, kCandTileBytes,
+                     &s.load_bar[as]);
+    }
+    const bool loaded = mbar_wait_parity(&s.load_bar[slot], (load_phase >> slot) & 1u);
+    load_phase ^= 1u << slot;
     if (!__syncthreads_and(loaded)) {
       ok = false;
       break;
     }
     float z0 = 0.f, z1 = 0.f;
-    if (!mlp_tile_forward(s.mlp, mma_phase, z0, z1, xbuf[buf])) {
+    if (!mlp_tile_forward(s.mlp, mma_phase, z0, z1, xbuf[slot])) {
       ok = false;
       break;
     }
     const uint32_t r = tile * kMlpTile + threadIdx.x;
     if (r < rows) {
-      const uint32_t slot = P.cand_slot[r];
+      const uint32_t hit = P.cand_slot[r];
       const bool seed = z0 >= P.mlp.seed_logit;
       const bool ext = !P.mlp.use_ext || z1 >= P.mlp.ext_logit;
-      if (!seed) P.windows[slot].x = 0xFFFFu;  // no h0 window: the search skips this h1
-      P.keep[slot] = static_cast<uint8_t>((seed ? 1u : 0u) | (ext ? 2u : 0u));
+      if (!seed) P.windows[hit].x = 0xFFFFu;  // no h0 window: the search skips this h1
+      P.keep[hit] = static_cast<uint8_t>((seed ? 1u : 0u) | (ext ? 2u : 0u));
     }
   }
-  if (!ok && threadIdx.x == 0) atomicOr(P.queue + 6, kErrorMlpTimeout);
-  // a bulk copy still in flight (timeout path) must land before the CTA exits
   if (!ok && threadIdx.x == 0) {
-    mbar_wait_parity(&s.load_bar[0], load_phase[0]);
-    mbar_wait_parity(&s.load_bar[1], load_phase[1]);
+    atomicOr(P.queue + 6, kErrorMlpTimeout);
+    // copies still in flight must land before the CTA exits: wait (bounded) on every slot
+    // whose issued copy has not been consumed
+    for (uint32_t j = 0; j < kScoreRing; ++j) mbar_wait_parity(&s.load_bar[j], (load_phase >> j) & 1u);
   }
   mlp_infer_teardown(s.mlp);
 }

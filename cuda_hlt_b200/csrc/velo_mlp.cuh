@@ -206,6 +206,7 @@ struct __align__(128) MlpInferSmem {
   uint64_t mbar;
   uint32_t tmem;
   float norm[32];
+  float w3f[2][kMlpHidden + 1];  // the output head (bf16 values as float), bias last
 };
 
 constexpr uint32_t kSbo1 = (kMlpK1 / 8) * 128;  // 256
@@ -222,6 +223,10 @@ __device__ __forceinline__ void mlp_infer_setup(MlpInferSmem& s, const MlpDevice
   load_canon(s.w1, mlp.w, kMlpHidden, kMlpK1);
   load_canon(s.w2, mlp.w + kMlpW1, kMlpHidden, kMlpK2);
   load_canon(s.w3, mlp.w + kMlpW1 + kMlpW2, kMlpOutPad, kMlpK2);
+  for (uint32_t i = threadIdx.x; i < 2 * (kMlpHidden + 1); i += blockDim.x) {
+    const uint32_t o = i / (kMlpHidden + 1), j = i % (kMlpHidden + 1);
+    s.w3f[o][j] = __bfloat162float(mlp.w[kMlpW1 + kMlpW2 + o * kMlpK2 + j]);
+  }
   umma_stage_barrier();
 }
 
@@ -296,6 +301,27 @@ __device__ __forceinline__ void mlp_hidden_epilogue(uint8_t* h, uint32_t taddr_r
   *reinterpret_cast<uint4*>(h + canon_off(row, 9, kSbo2)) = make_uint4(0u, 0u, 0u, 0u);
 }
 
+// The two-output head on the CUDA cores, fused into the epilogue of layer 2: relu of this
+// thread's 64 accumulators, rounded to bf16 as the tensor core would read them, dotted with
+// the bf16 head weights in fp32 (2.5% of the network's multiply-adds: a third tensor-core
+// round trip would cost more than the arithmetic).
+__device__ __forceinline__ void mlp_head_epilogue(const MlpInferSmem& s, uint32_t taddr_row, float& z0, float& z1)
+{
+  float v[64];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) tmem_ld16(taddr_row + 16 * c, *reinterpret_cast<float(*)[16]>(v + 16 * c));
+  tmem_ld_wait();
+  float a0 = s.w3f[0][kMlpHidden], a1 = s.w3f[1][kMlpHidden];
+#pragma unroll
+  for (int j = 0; j < 64; ++j) {
+    const float h = __bfloat162float(__float2bfloat16_rn(fmaxf(v[j], 0.f)));
+    a0 = fmaf(h, s.w3f[0][j], a0);
+    a1 = fmaf(h, s.w3f[1][j], a1);
+  }
+  z0 = a0;
+  z1 = a1;
+}
+
 // One layer of the inference tile: D(cols 0..n) = A * B^T, then wait.
 __device__ __forceinline__ bool mlp_layer(MlpInferSmem& s, uint32_t& phase, const uint8_t* a, uint32_t a_sbo,
                                           const uint8_t* b, uint32_t b_sbo, uint32_t k, uint32_t n)
@@ -317,13 +343,7 @@ __device__ __forceinline__ bool mlp_tile_forward(MlpInferSmem& s, uint32_t& phas
   if (!mlp_layer(s, phase, x ? x : s.x, kSbo1, s.w1, kSbo1, kMlpK1, kMlpHidden)) return false;
   mlp_hidden_epilogue(s.h, taddr_row);
   if (!mlp_layer(s, phase, s.h, kSbo2, s.w2, kSbo2, kMlpK2, kMlpHidden)) return false;
-  mlp_hidden_epilogue(s.h, taddr_row);
-  if (!mlp_layer(s, phase, s.h, kSbo2, s.w3, kSbo2, kMlpK2, kMlpOutPad)) return false;
-  float v[16];
-  tmem_ld16(taddr_row, v);
-  tmem_ld_wait();
-  z0 = v[0];
-  z1 = v[1];
+  mlp_head_epilogue(s, taddr_row, z0, z1);
   return true;
 }
 
