@@ -168,20 +168,22 @@ def load_scorer(args):
     if not args.retrain and os.path.exists(path):
         w = mlp.load_weights(path)
         return w, {"weights": os.path.relpath(path, ROOT), "trained": "committed", "seed_threshold": w.seed_threshold,
-                   "max_event_clusters": w.max_event_clusters}
+                   "min_pairs": w.min_pairs, "max_event_clusters": w.max_event_clusters}
     log("training the scorer (train_scorer pipeline, 1M samples, 4 epochs)")
     t0 = time.time()
     trainer = mlp.MlpTrainer(1_000_000, seed=1)
-    held, max_clusters, _, _ = train_scorer.collect_training(trainer, 1_000_000, os.cpu_count() or 1)
+    threads = os.cpu_count() or 1
+    held, max_clusters, _, next_event = train_scorer.collect_training(trainer, 1_000_000, threads)
     trainer.normalize()
     trainer.train(4, 16384, 2e-3)
     w = trainer.weights()
     trainer.close()
     w.max_event_clusters = max_clusters
-    w.seed_threshold = 0.1
     w.ext_threshold = 0.0
-    return w, {"trained": f"in bench: {held} samples, {time.time() - t0:.1f}s", "seed_threshold": 0.1,
-               "max_event_clusters": max_clusters}
+    val = events.generate_config("mlp_train", n_events=8192, first_event=next_event, threads=threads, with_mc=True)
+    (w.seed_threshold, w.min_pairs), _, _ = train_scorer.choose_operating_point(w, val, 0.001)
+    return w, {"trained": f"in bench: {held} samples, {time.time() - t0:.1f}s", "seed_threshold": w.seed_threshold,
+               "min_pairs": w.min_pairs, "max_event_clusters": max_clusters}
 
 
 def time_form(vcs, streams, batch_ptrs, args, world, dist, torch, local_rank):

@@ -73,7 +73,7 @@ class VeloMlpWeights(C.Structure):
         ("seed_threshold", C.c_float),
         ("ext_threshold", C.c_float),
         ("max_event_clusters", C.c_uint32),
-        ("reserved", C.c_uint32),
+        ("min_pairs", C.c_uint32),
     ]
 
 

@@ -17,7 +17,8 @@
 //                          cleared, so the search never sees it; keep bits per hit (bit 0
 //                          seed keep, bit 1 extension keep) are kept for the outputs.
 // Events above the scorer's occupancy range append no candidates (the plain search) and get
-// VELO_STATUS_MLP_FALLBACK.
+// VELO_STATUS_MLP_FALLBACK. Seeds with fewer than min_pairs (h0, h2) combinations are not
+// appended either: they stay seeds, as scoring them would cost more than their pair loop.
 #pragma once
 #include "velo_mlp.cuh"
 
@@ -87,7 +88,8 @@ __global__ void __launch_bounds__(kFillThreads) fill_candidates_kernel(ChainPoin
         if (kPruned) {
           const bool cand = valid && f0 != -1 && f2 != -1;
           if (valid) P.keep[base + h] = cand ? 3u : 2u;  // candidates: verdict from score_candidates
-          const bool append = cand && !fallback;
+          // seeds whose pair loop is cheaper than their scoring stay kept, unscored
+          const bool append = cand && !fallback && static_cast<uint32_t>((l0 - f0) * (l2 - f2)) >= P.mlp.min_pairs;
           // one atomic per warp for the rows of its candidates
           const uint32_t bal = __ballot_sync(0xFFFFFFFFu, append);
           uint32_t row0 = 0;
@@ -153,6 +155,8 @@ __global__ void __launch_bounds__(kMlpTile) score_candidates_kernel(ChainPointer
       bulk_load_smem(xbuf[as], P.cand_feat + static_cast<size_t>(ahead) * kCandTileBytes, kCandTileBytes,
                      &s.load_bar[as]);
     }
+    const uint32_t r = tile * kMlpTile + threadIdx.x;
+    const uint32_t hit = r < rows ? P.cand_slot[r] : 0u;  // issued early: used after the MMAs
     const bool loaded = mbar_wait_parity(&s.load_bar[slot], (load_phase >> slot) & 1u);
     load_phase ^= 1u << slot;
     if (!__syncthreads_and(loaded)) {
@@ -164,9 +168,7 @@ __global__ void __launch_bounds__(kMlpTile) score_candidates_kernel(ChainPointer
       ok = false;
       break;
     }
-    const uint32_t r = tile * kMlpTile + threadIdx.x;
     if (r < rows) {
-      const uint32_t hit = P.cand_slot[r];
       const bool seed = z0 >= P.mlp.seed_logit;
       const bool ext = !P.mlp.use_ext || z1 >= P.mlp.ext_logit;
       if (!seed) P.windows[hit].x = 0xFFFFu;  // no h0 window: the search skips this h1

@@ -53,6 +53,7 @@ struct MlpDevice {
   float ext_logit;         // hit kept as an extension candidate when logit 1 >= ext_logit
   uint32_t use_ext;        // extension pruning on
   uint32_t max_hits;       // events with more clusters fall back to the plain search
+  uint32_t min_pairs;      // seeds with fewer (h0, h2) pairs are kept unscored
 };
 
 // Clusters after the phi sort: position and phi of a cluster in one 16-byte record (one

@@ -197,20 +197,24 @@ __device__ __forceinline__ bool umma_wait(uint64_t* mbar, uint32_t& phase)
 // ---------------------------------------------------------------------------------
 // Inference on 128-row tiles (128 threads, one row each)
 // ---------------------------------------------------------------------------------
+// Inference keeps the hidden layer at K = 64 (the layer-2 bias is added in fp32 in the
+// epilogue: the same bf16 value the training's ones column multiplies by 1) and computes the
+// two-output head on the CUDA cores, so it needs neither the padded H columns nor a W3 tile.
 struct __align__(128) MlpInferSmem {
   uint8_t w1[kMlpW1 * 2];
-  uint8_t w2[kMlpW2 * 2];
-  uint8_t w3[kMlpW3 * 2];
+  uint8_t w2[kMlpHidden * kMlpHidden * 2];
   uint8_t x[kMlpTile * kMlpK1 * 2];
-  uint8_t h[kMlpTile * kMlpK2 * 2];
+  uint8_t h[kMlpTile * kMlpHidden * 2];
   uint64_t mbar;
   uint32_t tmem;
   float norm[32];
-  float w3f[2][kMlpHidden + 1];  // the output head (bf16 values as float), bias last
+  float b2[kMlpHidden];
+  float2 w3[kMlpHidden + 1];  // head weights (output 0, output 1) per hidden unit, bias last
 };
 
-constexpr uint32_t kSbo1 = (kMlpK1 / 8) * 128;  // 256
-constexpr uint32_t kSbo2 = (kMlpK2 / 8) * 128;  // 1280
+constexpr uint32_t kSbo1 = (kMlpK1 / 8) * 128;      // 256
+constexpr uint32_t kSbo2 = (kMlpK2 / 8) * 128;      // 1280 (training tiles, K = 80)
+constexpr uint32_t kSboH = (kMlpHidden / 8) * 128;  // 1024 (inference hidden tile, K = 64)
 constexpr uint32_t kMlpInferTmemCols = 64;       // D1, D2 and D3 share columns 0..63
 constexpr uint32_t kMlpInferSmem = sizeof(MlpInferSmem) + 128;  // dynamic size, 128-byte aligned
 
@@ -221,11 +225,16 @@ __device__ __forceinline__ void mlp_infer_setup(MlpInferSmem& s, const MlpDevice
   if (threadIdx.x == 0) mbar_init1(&s.mbar);
   if (threadIdx.x < 32) s.norm[threadIdx.x] = mlp.norm[threadIdx.x];
   load_canon(s.w1, mlp.w, kMlpHidden, kMlpK1);
-  load_canon(s.w2, mlp.w + kMlpW1, kMlpHidden, kMlpK2);
-  load_canon(s.w3, mlp.w + kMlpW1 + kMlpW2, kMlpOutPad, kMlpK2);
-  for (uint32_t i = threadIdx.x; i < 2 * (kMlpHidden + 1); i += blockDim.x) {
-    const uint32_t o = i / (kMlpHidden + 1), j = i % (kMlpHidden + 1);
-    s.w3f[o][j] = __bfloat162float(mlp.w[kMlpW1 + kMlpW2 + o * kMlpK2 + j]);
+  // W2 without its bias column: rows of 80, first 64 columns
+  for (uint32_t c = threadIdx.x; c < kMlpHidden * 8; c += blockDim.x) {
+    const uint32_t row = c / 8, kb = c % 8;
+    *reinterpret_cast<uint4*>(s.w2 + canon_off(row, kb, kSboH)) =
+      *reinterpret_cast<const uint4*>(mlp.w + kMlpW1 + row * kMlpK2 + kb * 8);
+  }
+  for (uint32_t j = threadIdx.x; j <= kMlpHidden; j += blockDim.x) {
+    const __nv_bfloat16* w3 = mlp.w + kMlpW1 + kMlpW2;
+    s.w3[j] = make_float2(__bfloat162float(w3[j]), __bfloat162float(w3[kMlpK2 + j]));
+    if (j < kMlpHidden) s.b2[j] = __bfloat162float(mlp.w[kMlpW1 + j * kMlpK2 + kMlpHidden]);
   }
   umma_stage_barrier();
 }
@@ -280,7 +289,7 @@ __device__ __forceinline__ void mlp_store_features(MlpInferSmem& s, const float 
 }
 
 // Reads this thread's 64 accumulator columns, applies ReLU and writes the bf16 row of H
-// (with the bias column).
+// (inference layout: 64 columns, no bias column).
 __device__ __forceinline__ void mlp_hidden_epilogue(uint8_t* h, uint32_t taddr_row)
 {
   const uint32_t row = threadIdx.x;
@@ -295,10 +304,8 @@ __device__ __forceinline__ void mlp_hidden_epilogue(uint8_t* h, uint32_t taddr_r
     q.y = pack_bf16x2(fmaxf(v[8 * kb + 2], 0.f), fmaxf(v[8 * kb + 3], 0.f));
     q.z = pack_bf16x2(fmaxf(v[8 * kb + 4], 0.f), fmaxf(v[8 * kb + 5], 0.f));
     q.w = pack_bf16x2(fmaxf(v[8 * kb + 6], 0.f), fmaxf(v[8 * kb + 7], 0.f));
-    *reinterpret_cast<uint4*>(h + canon_off(row, kb, kSbo2)) = q;
+    *reinterpret_cast<uint4*>(h + canon_off(row, kb, kSboH)) = q;
   }
-  *reinterpret_cast<uint4*>(h + canon_off(row, 8, kSbo2)) = make_uint4(0x3F80u, 0u, 0u, 0u);  // bf16 1.0
-  *reinterpret_cast<uint4*>(h + canon_off(row, 9, kSbo2)) = make_uint4(0u, 0u, 0u, 0u);
 }
 
 // The two-output head on the CUDA cores, fused into the epilogue of layer 2: relu of this
@@ -311,12 +318,14 @@ __device__ __forceinline__ void mlp_head_epilogue(const MlpInferSmem& s, uint32_
 #pragma unroll
   for (int c = 0; c < 4; ++c) tmem_ld16(taddr_row + 16 * c, *reinterpret_cast<float(*)[16]>(v + 16 * c));
   tmem_ld_wait();
-  float a0 = s.w3f[0][kMlpHidden], a1 = s.w3f[1][kMlpHidden];
+  const float2 bias = s.w3[kMlpHidden];
+  float a0 = bias.x, a1 = bias.y;
 #pragma unroll
   for (int j = 0; j < 64; ++j) {
-    const float h = __bfloat162float(__float2bfloat16_rn(fmaxf(v[j], 0.f)));
-    a0 = fmaf(h, s.w3f[0][j], a0);
-    a1 = fmaf(h, s.w3f[1][j], a1);
+    const float h = __bfloat162float(__float2bfloat16_rn(fmaxf(v[j] + s.b2[j], 0.f)));
+    const float2 w = s.w3[j];
+    a0 = fmaf(h, w.x, a0);
+    a1 = fmaf(h, w.y, a1);
   }
   z0 = a0;
   z1 = a1;
@@ -342,7 +351,7 @@ __device__ __forceinline__ bool mlp_tile_forward(MlpInferSmem& s, uint32_t& phas
   const uint32_t taddr_row = s.tmem + ((threadIdx.x & ~31u) << 16);
   if (!mlp_layer(s, phase, x ? x : s.x, kSbo1, s.w1, kSbo1, kMlpK1, kMlpHidden)) return false;
   mlp_hidden_epilogue(s.h, taddr_row);
-  if (!mlp_layer(s, phase, s.h, kSbo2, s.w2, kSbo2, kMlpK2, kMlpHidden)) return false;
+  if (!mlp_layer(s, phase, s.h, kSboH, s.w2, kSboH, kMlpHidden, kMlpHidden)) return false;
   mlp_head_epilogue(s, taddr_row, z0, z1);
   return true;
 }

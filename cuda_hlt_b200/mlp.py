@@ -30,7 +30,8 @@ def weights_to_dict(w):
     return dict(mean=np.ctypeslib.as_array(w.mean).copy(), inv_std=np.ctypeslib.as_array(w.inv_std).copy(),
                 w1=np.ctypeslib.as_array(w.w1).copy(), w2=np.ctypeslib.as_array(w.w2).copy(),
                 w3=np.ctypeslib.as_array(w.w3).copy(), seed_threshold=float(w.seed_threshold),
-                ext_threshold=float(w.ext_threshold), max_event_clusters=int(w.max_event_clusters))
+                ext_threshold=float(w.ext_threshold), max_event_clusters=int(w.max_event_clusters),
+                min_pairs=int(w.min_pairs))
 
 
 def dict_to_weights(d):
@@ -40,6 +41,7 @@ def dict_to_weights(d):
     w.seed_threshold = d.get("seed_threshold", 0.5)
     w.ext_threshold = d.get("ext_threshold", 0.0)
     w.max_event_clusters = d.get("max_event_clusters", 0xFFFFFFFF)
+    w.min_pairs = d.get("min_pairs", 0)
     return w
 
 

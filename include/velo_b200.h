@@ -196,7 +196,9 @@ int velo_sync(VeloCtx* ctx, uint32_t* total_tracks, uint32_t* total_track_hits, 
  * 1 ("extension keep") that h1 is the fourth or a later hit of one. In VELO_MODE_PRUNED the
  * search seeds only from h1 with p0 >= seed_threshold and, when ext_threshold > 0,
  * forwards only onto hits with p1 >= ext_threshold; events with more than
- * max_event_clusters clusters run the plain search (VELO_STATUS_MLP_FALLBACK).
+ * max_event_clusters clusters run the plain search (VELO_STATUS_MLP_FALLBACK). Seeds with
+ * fewer than min_pairs (h0, h2) combinations to test are kept without scoring: the scorer
+ * costs the same for every candidate, the search only for the combinations it tests.
  * Inference and training run on the tensor cores in bf16 with fp32 accumulation. */
 typedef struct VeloMlpWeights {
   float mean[12];               /* feature normalisation: (f - mean) * inv_std */
@@ -207,7 +209,7 @@ typedef struct VeloMlpWeights {
   float seed_threshold;         /* probability */
   float ext_threshold;          /* probability; 0 disables extension pruning */
   uint32_t max_event_clusters;  /* occupancy limit of the trained range */
-  uint32_t reserved;
+  uint32_t min_pairs;           /* score only seeds with |h0 window| x |h2 window| >= this */
 } VeloMlpWeights;
 
 /* Loads the scorer (weights_host -> VeloMlpWeights, bytes == sizeof(VeloMlpWeights));
