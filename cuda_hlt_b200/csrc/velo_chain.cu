@@ -15,6 +15,7 @@
 #include "velo_ctx.hpp"
 #include "velo_decode.cuh"
 #include "velo_fill.cuh"
+#include "velo_order.cuh"
 #include "velo_search.cuh"
 #include "velo_search_block.cuh"
 #include "velo_consolidate.cuh"
@@ -63,7 +64,7 @@ struct VeloCtx {
   uint32_t *d_atomics = nullptr, *d_track_hit_number = nullptr, *d_event_hit_offset = nullptr;
   char *d_track_hits_out = nullptr, *d_states = nullptr, *d_kalman = nullptr;
   uint32_t* d_queue = nullptr;
-  uint32_t *d_warp_events = nullptr, *d_block_events = nullptr;
+  uint32_t *d_warp_events = nullptr, *d_block_events = nullptr, *d_event_order = nullptr;
   uint32_t block_threshold = 0;  // clusters above which an event takes the block search
   uint32_t* h_totals = nullptr;  // pinned [4]
   cudaStream_t last_stream = nullptr;
@@ -130,7 +131,7 @@ void free_all(VeloCtx* c)
                   c->d_event_hits, c->d_status, c->d_track_n, c->d_track_hits, c->d_tracklets, c->d_weak, c->d_ttf,
                   c->d_event_tracks, c->d_event_track_hits, c->d_atomics, c->d_track_hit_number,
                   c->d_event_hit_offset, c->d_track_hits_out, c->d_states, c->d_kalman, c->d_queue,
-                  c->d_warp_events, c->d_block_events};
+                  c->d_warp_events, c->d_block_events, c->d_event_order};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c->h_totals) cudaFreeHost(c->h_totals);
@@ -187,6 +188,7 @@ ChainPointers pointers(VeloCtx* c, const void* raw, const uint64_t* offsets, uin
   P.hit_capacity = c->hit_capacity;
   P.queue = c->d_queue;
   P.warp_events = c->d_warp_events;
+  P.event_order = c->d_event_order;
   P.block_events = c->d_block_events;
   P.block_threshold = c->block_threshold;
   P.mlp = c->mlp;
@@ -230,10 +232,12 @@ int launch_chain(VeloCtx* c, const ChainPointers& P, cudaStream_t s, bool captur
   {
     // both mappings: each kernel drains its own event list (routed by the decode kernel)
     if (c->block_threshold > 0) {
+      order_events_kernel<<<1, kOrderThreads, 0, s>>>(P);
+      VCK(cudaGetLastError());
       const uint32_t blocks = std::min<uint32_t>((n + 3) / 4, c->search_blocks);
       search_kernel<4><<<blocks, 128, 0, s>>>(P);
       VCK(cudaGetLastError());
-      ++c->launches;
+      c->launches += 2;
     }
     if (c->block_threshold < kEventHitCap) {
       const uint32_t blocks = std::min<uint32_t>(n, c->search_block_blocks);
@@ -330,6 +334,7 @@ int velo_create(const VeloConfig* cfg, const void* geometry, size_t geometry_byt
   ok &= dalloc(c->d_queue, 8) == cudaSuccess;
   ok &= dalloc(c->d_warp_events, N) == cudaSuccess;
   ok &= dalloc(c->d_block_events, N) == cudaSuccess;
+  ok &= dalloc(c->d_event_order, N) == cudaSuccess;
   ok &= cudaMallocHost(reinterpret_cast<void**>(&c->h_totals), 4 * sizeof(uint32_t) + 8) == cudaSuccess;
   if (!ok) return fail(VELO_ERR_CUDA);
   uint8_t pat[256], sizes[256];

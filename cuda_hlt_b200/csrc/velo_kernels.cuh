@@ -111,6 +111,7 @@ struct ChainPointers {
   // [4] / [5] sizes of the warp / block event lists, [6] error bits, [7] candidate rows
   uint32_t* queue;             // [8]
   uint32_t* warp_events;       // [N] events routed to the warp-per-event search
+  uint32_t* event_order;       // [N] warp_events, largest first: the warp search's queue order
   uint32_t* block_events;      // [N] events routed to the block-per-event search
   uint32_t block_threshold;    // events with more clusters than this go to the block search
   // learned pruning (read when keep != nullptr)

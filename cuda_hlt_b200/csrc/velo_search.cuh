@@ -1,4 +1,5 @@
-// Kernel 3 of the chain: search_by_triplet, one warp per event (persistent, queue).
+// Kernel 3 of the chain: search_by_triplet, one warp per event (persistent, queue), events
+// handed out largest first (order_events_kernel, velo_order.cuh).
 //
 // The module loop, forwarding and weak-track rules are those of the reference
 // (ProcessModules.cu:8-163, TrackForwarding.cu:41-181, TrackSeeding.cu:7-200,
@@ -210,7 +211,7 @@ __global__ void __launch_bounds__(WPB * 32) search_kernel(ChainPointers P)
     if (lane == 0) q = atomicAdd(P.queue + 1, 1u);
     q = __shfl_sync(0xFFFFFFFFu, q, 0);
     if (q >= P.queue[4]) break;
-    const uint32_t e = P.warp_events[q];
+    const uint32_t e = P.event_order[q];
     const uint32_t nhits = P.event_hits[e];
     const uint32_t status = P.status[e];
     const uint32_t base = P.event_hit_base[e];
