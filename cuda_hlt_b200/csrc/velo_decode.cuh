@@ -256,30 +256,34 @@ __device__ __forceinline__ void bitonic_cx(unsigned long long& a, unsigned long 
   b = up ? hi : lo;
 }
 
-// Bitonic sort of 32 * 4 keys held 4 per lane (element j * 32 + lane), first `size`
-// elements (a power of two, 32..128). Every register index is a compile-time constant, so
+// Bitonic sort of 32 * PER keys held PER per lane, element lane * PER + j in key[j]
+// (the input may sit in any slots: only the sorted order is read back this way). The
+// exchanges between elements less than PER apart stay inside a lane, the others take one
+// shuffle per key; loops unrolled, so every register index is a compile-time constant and
 // the keys stay in registers.
-__device__ __forceinline__ void warp_register_sort(unsigned long long (&key)[4], uint32_t size)
+template<uint32_t PER>
+__device__ __forceinline__ void warp_register_sort(unsigned long long (&key)[4])
 {
   const uint32_t lane = lane_id();
-  const uint32_t per = size >> 5;
-  for (uint32_t k = 2; k <= size; k <<= 1) {
-    for (uint32_t d = k >> 1; d > 0; d >>= 1) {
-      if (d == 64) {  // registers j and j + 2 (size 128)
-        bitonic_cx(key[0], key[2], ((0 * 32 + lane) & k) == 0);
-        bitonic_cx(key[1], key[3], ((1 * 32 + lane) & k) == 0);
-      } else if (d == 32) {  // registers j and j + 1
-        bitonic_cx(key[0], key[1], ((0 * 32 + lane) & k) == 0);
-        if (per == 4) bitonic_cx(key[2], key[3], ((2 * 32 + lane) & k) == 0);
-      } else {
 #pragma unroll
-        for (uint32_t j = 0; j < 4; ++j) {
-          if (j >= per) continue;
-          const unsigned long long p = __shfl_xor_sync(0xFFFFFFFFu, key[j], d);
-          const bool lower = (lane & d) == 0;
-          const bool up = ((j * 32 + lane) & k) == 0;
+  for (uint32_t k = 2; k <= 32 * PER; k <<= 1) {
+#pragma unroll
+    for (uint32_t d = k >> 1; d > 0; d >>= 1) {
+      if (d >= PER) {
+        const uint32_t ld = d / PER;  // partner lane distance
+        const bool lower = (lane & ld) == 0;
+#pragma unroll
+        for (uint32_t j = 0; j < PER; ++j) {
+          const unsigned long long p = __shfl_xor_sync(0xFFFFFFFFu, key[j], ld);
+          const bool up = ((lane * PER + j) & k) == 0;
           key[j] = (lower == up) ? min(key[j], p) : max(key[j], p);
         }
+      } else if (d == 2) {  // PER == 4: registers j and j + 2
+        bitonic_cx(key[0], key[2], ((lane * PER + 0) & k) == 0);
+        bitonic_cx(key[1], key[3], ((lane * PER + 1) & k) == 0);
+      } else {  // d == 1: registers j and j + 1
+        bitonic_cx(key[0], key[1], ((lane * PER + 0) & k) == 0);
+        if (PER == 4) bitonic_cx(key[2], key[3], ((lane * PER + 2) & k) == 0);
       }
     }
   }
@@ -494,19 +498,20 @@ __global__ void __launch_bounds__(W * 32) decode_cluster_sort_kernel(ChainPointe
       uint8_t* dst_size = P.hit_size + p0;
       if (n > kMaxHitsPerModule && lane == 0) atomicOr(&sh.flags, kStatusModuleOverflow);
       if (n <= kRegSortMax) {
-        uint32_t size = 32;
-        while (size < n) size <<= 1;
+        const uint32_t per = n > 64 ? 4 : n > 32 ? 2 : 1;
         unsigned long long key[4];
 #pragma unroll
-        for (uint32_t j = 0; j < 4; ++j) {
+        for (uint32_t j = 0; j < 4; ++j) {  // coalesced loads; slots j >= per hold padding only
           const uint32_t i = j * 32 + lane;
           key[j] = i < n ? cluster_key(src, src_id, i) : ~0ull;
         }
-        if (n > 1) warp_register_sort(key, size);
+        if (per == 4) warp_register_sort<4>(key);
+        else if (per == 2) warp_register_sort<2>(key);
+        else if (n > 1) warp_register_sort<1>(key);
 #pragma unroll
         for (uint32_t j = 0; j < 4; ++j) {
-          const uint32_t i = j * 32 + lane;
-          if (i < n) {
+          const uint32_t i = lane * per + j;  // rank of key[j]
+          if (j < per && i < n) {
             const uint32_t from = static_cast<uint32_t>(key[j] & 0xFFFu);
             const uint32_t id = src_id[from];
             dst[i] = src[from];
