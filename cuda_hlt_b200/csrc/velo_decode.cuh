@@ -248,12 +248,14 @@ __device__ __forceinline__ unsigned long long cluster_key(const float4* src, con
          (static_cast<unsigned long long>(src_id[i] & 0xFFFFFu) << 12) | i;
 }
 
-// Compare-exchange of elements a (lower index) and b in bitonic order `up`.
+// Compare-exchange of elements a (lower index) and b in bitonic order `up`: one 64-bit
+// comparison and a conditional swap (keys are distinct: the slot is part of the key).
 __device__ __forceinline__ void bitonic_cx(unsigned long long& a, unsigned long long& b, bool up)
 {
-  const unsigned long long lo = min(a, b), hi = max(a, b);
-  a = up ? lo : hi;
-  b = up ? hi : lo;
+  const bool swap = (b < a) == up;
+  const unsigned long long t = a;
+  a = swap ? b : a;
+  b = swap ? t : b;
 }
 
 // Bitonic sort of 32 * PER keys held PER per lane, element lane * PER + j in key[j]
@@ -276,7 +278,9 @@ __device__ __forceinline__ void warp_register_sort(unsigned long long (&key)[4])
         for (uint32_t j = 0; j < PER; ++j) {
           const unsigned long long p = __shfl_xor_sync(0xFFFFFFFFu, key[j], ld);
           const bool up = ((lane * PER + j) & k) == 0;
-          key[j] = (lower == up) ? min(key[j], p) : max(key[j], p);
+          // keep the smaller of the pair (lower lane of an ascending pair, or upper lane of a
+          // descending one) or the larger
+          key[j] = ((p < key[j]) == (lower == up)) ? p : key[j];
         }
       } else if (d == 2) {  // PER == 4: registers j and j + 2
         bitonic_cx(key[0], key[2], ((lane * PER + 0) & k) == 0);
