@@ -63,15 +63,15 @@ __device__ __forceinline__ SpWindow gather_window(const uint32_t* bank, uint32_t
 {
   SpWindow w{{0u, 0u, 0u}, 0u, 0u, 0u, 0u, 0u};
   if (sorted) {
-    const int32_t rlo = max(r - 2, 0), rhi = min(r + 1, 63);
-#pragma unroll 1
-    for (int32_t col = max(c - 1, 0); col <= min(c + 1, 511); ++col) {
-      const uint32_t a_hi = (static_cast<uint32_t>(col) << 6) | rhi;
-      for (uint32_t i = bank_lower_bound(bank, count, (static_cast<uint32_t>(col) << 6) | rlo); i < count; ++i) {
-        const uint32_t o = __ldg(bank + i);
-        if (sp_addr(o) > a_hi) break;
-        window_add(w, o, r, c);
-      }
+    // the three columns are adjacent in address order (column << 6 | row): one search and
+    // one scan over [(c - 1, r - 2), (c + 1, r + 1)]; the rows outside [r - 2, r + 1] that
+    // the scan also meets are rejected by window_add
+    const uint32_t a_lo = (static_cast<uint32_t>(max(c - 1, 0)) << 6) | static_cast<uint32_t>(max(r - 2, 0));
+    const uint32_t a_hi = (static_cast<uint32_t>(min(c + 1, 511)) << 6) | static_cast<uint32_t>(min(r + 1, 63));
+    for (uint32_t i = bank_lower_bound(bank, count, a_lo); i < count; ++i) {
+      const uint32_t o = __ldg(bank + i);
+      if (sp_addr(o) > a_hi) break;
+      window_add(w, o, r, c);
     }
   } else {
     for (uint32_t i = 0; i < count; ++i) window_add(w, __ldg(bank + i), r, c);
