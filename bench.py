@@ -138,7 +138,7 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
-TRAFFIC_SUMMARIES = ["velo_chain_batched_8192_warp_ncu.md", "velo_chain_batched_8192_block1536_ncu.md"]
+TRAFFIC_SUMMARIES = ["velo_chain_pruned_1m_8192_ncu.md", "velo_chain_batched_8192_block1536_ncu.md"]
 
 
 def load_traffic():
