@@ -5,7 +5,7 @@ nu ~ U(2,20) workload.
 python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 One step = one pass of the chain over the rank's 1,000,000 synthetic events (seed 4,
-events rank*1000000 ...), in batches of 16,384 events (one CUDA graph per batch). Both
+events rank*1000000 ...), in batches of 32,768 events (one CUDA graph per batch). Both
 forms run on the same device-resident input: the plain chain (reference semantics) and
 the pruned chain (learned seed scorer; events above the scorer's trained occupancy fall
 back to the plain search). Events are independent, so ranks process disjoint event
@@ -42,8 +42,9 @@ METRIC = "VELO events/s on 1 B200, MLP-pruned vs plain at ≤0.2% eff loss; % HB
 UNIT = "events/s"
 WORKLOAD = "pruned_1m"
 N_EVENTS = 1_000_000
-BUCKET = 16384
+BUCKET = 32768   # events per batch (one CUDA graph); --batch
 CHUNK = 4 * BUCKET
+SIDE_BATCH = 16384  # batches of the MC-quality and reference-kernel legs
 
 
 def log(*a):
@@ -261,8 +262,8 @@ def run_quality(weights, n, threads):
     """Long-track efficiency and ghost rate of both forms against generator truth on the
     first n events of the workload (with MC truth)."""
     rows = {"plain": [], "pruned": []}
-    for a in range(0, n, BUCKET):
-        m = min(BUCKET, n - a)
+    for a in range(0, n, SIDE_BATCH):
+        m = min(SIDE_BATCH, n - a)
         b = events.generate_config(WORKLOAD, n_events=m, first_event=a, threads=threads, with_mc=True)
         for name, mode in (("plain", chain.MODE_PLAIN), ("pruned", chain.MODE_PRUNED)):
             vc = chain.VeloChain(max_events=m, max_raw_bytes=int(b.raw.size) + 4096)
@@ -416,8 +417,10 @@ def run_e2e(args, chunks, plan, local_rank, torch, world, dist, threshold, weigh
         vc.set_mode(chain.MODE_PRUNED)
     streams = [torch.cuda.Stream(device=local_rank) for _ in range(2)]
     # pinned result buffers per context: atomics, hit numbers, hits SoA, Kalman states
-    cap_t = 400 * BUCKET
-    cap_h = 16 * cap_t
+    # (the workload averages 166 tracks and 1,340 track hits per event; a batch beyond these
+    # capacities raises before any copy)
+    cap_t = 300 * BUCKET
+    cap_h = 12 * cap_t
     outs = [dict(atomics=torch.empty(2 * BUCKET + 1, dtype=torch.int32, pin_memory=True),
                  thn=torch.empty(cap_t + 1, dtype=torch.int32, pin_memory=True),
                  hits=torch.empty(16 * cap_h, dtype=torch.uint8, pin_memory=True),
@@ -435,6 +438,9 @@ def run_e2e(args, chunks, plan, local_rank, torch, world, dist, threshold, weigh
                                  (o["thn"], vc.out.track_hit_number, 4 * (t + 1)),
                                  (o["hits"], vc.out.track_hits, 16 * h),
                                  (o["kal"], vc.out.kalman_states, 49 * t)):
+            if nbytes > buf.numel() * buf.element_size():
+                raise RuntimeError(f"e2e: batch {k} needs {nbytes} bytes, pinned buffer holds "
+                                   f"{buf.numel() * buf.element_size()}")
             if nbytes:
                 chain._check(lib.velo_download_async(vc.ctx, C.c_void_p(buf.data_ptr()), C.c_void_p(src), nbytes,
                                                      C.c_void_p(s.cuda_stream)), "velo_download_async")
@@ -558,6 +564,7 @@ def run_reference(args):
 
 
 def main():
+    global BUCKET, CHUNK
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -568,10 +575,12 @@ def main():
     ap.add_argument("--reference-sample", type=int, default=8192)
     ap.add_argument("--quality-events", type=int, default=32768, help="MC-checked events of the workload head")
     ap.add_argument("--streams", type=int, default=2, help="contexts / streams that batches alternate between")
+    ap.add_argument("--batch", type=int, default=BUCKET, help="events per batch (one CUDA graph per batch)")
     ap.add_argument("--weights", default=None, help="scorer weights (default: the committed file)")
     ap.add_argument("--retrain", action="store_true", help="train the scorer here instead of loading it")
     ap.add_argument("--no-extras", action="store_true", help="skip the CPU baseline and reference-GPU legs")
     args = ap.parse_args()
+    BUCKET, CHUNK = args.batch, 4 * args.batch
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
@@ -599,7 +608,7 @@ def main():
             sample = None
         if world == 1:
             try:
-                b0 = chunks[0].subset(0, min(BUCKET, chunks[0].n_events))
+                b0 = chunks[0].subset(0, min(SIDE_BATCH, chunks[0].n_events))
                 result["reference_gpu_b200"] = reference_gpu(b0)
             except Exception as ex:
                 result["reference_gpu_b200"] = {"error": str(ex)}
