@@ -45,6 +45,7 @@ N_EVENTS = 1_000_000
 BUCKET = 32768   # events per batch (one CUDA graph); --batch
 CHUNK = 4 * BUCKET
 SIDE_BATCH = 16384  # batches of the MC-quality and reference-kernel legs
+E2E_CONTEXTS = 3    # contexts (and streams) in rotation in the end-to-end leg
 
 
 def log(*a):
@@ -397,9 +398,10 @@ def run_ours(args, rank, world, local_rank):
 
 
 def run_e2e(args, chunks, plan, local_rank, torch, world, dist, threshold, weights):
-    """velo_run_host from pinned memory, two contexts alternating on two streams so that
-    the copies of one batch overlap the kernels of the other; outputs read back to pinned
-    host buffers every batch."""
+    """velo_run_host from pinned memory, E2E_CONTEXTS contexts in rotation, each on its own
+    stream, so that the upload of one batch, the kernels of the next and the read-back of a
+    third overlap (uploads and read-backs use the host link in opposite directions); outputs
+    read back to pinned host buffers every batch."""
     import ctypes as C
     cudart = torch.cuda.cudart()
     for c in chunks:
@@ -409,29 +411,30 @@ def run_e2e(args, chunks, plan, local_rank, torch, world, dist, threshold, weigh
         o = chunks[ci].offsets[a:b + 1]
         offs.append(np.ascontiguousarray(o - o[0], dtype=np.uint64))
     max_batch_bytes = max(int(chunks[ci].offsets[b] - chunks[ci].offsets[a]) for ci, a, b in plan)
+    nctx = E2E_CONTEXTS
     ctxs = [chain.VeloChain(max_events=BUCKET, max_raw_bytes=max_batch_bytes + 4096, device=local_rank)
-            for _ in range(2)]
+            for _ in range(nctx)]
     for vc in ctxs:
         vc.set_block_threshold(threshold)
         vc.set_mlp(weights)
         vc.set_mode(chain.MODE_PRUNED)
-    streams = [torch.cuda.Stream(device=local_rank) for _ in range(2)]
+    streams = [torch.cuda.Stream(device=local_rank) for _ in range(nctx)]
     # pinned result buffers per context: atomics, hit numbers, hits SoA, Kalman states
     # (the workload averages 166 tracks and 1,340 track hits per event; a batch beyond these
     # capacities raises before any copy)
-    cap_t = 300 * BUCKET
-    cap_h = 12 * cap_t
+    cap_t = 250 * BUCKET
+    cap_h = 10 * cap_t
     outs = [dict(atomics=torch.empty(2 * BUCKET + 1, dtype=torch.int32, pin_memory=True),
                  thn=torch.empty(cap_t + 1, dtype=torch.int32, pin_memory=True),
                  hits=torch.empty(16 * cap_h, dtype=torch.uint8, pin_memory=True),
-                 kal=torch.empty(52 * cap_t, dtype=torch.uint8, pin_memory=True)) for _ in range(2)]
+                 kal=torch.empty(52 * cap_t, dtype=torch.uint8, pin_memory=True)) for _ in range(nctx)]
     lib = ctxs[0].lib
 
     d2h = [0]
     h2d = [0]
 
     def fetch(k):
-        vc, o, s = ctxs[k % 2], outs[k % 2], streams[k % 2]
+        vc, o, s = ctxs[k % nctx], outs[k % nctx], streams[k % nctx]
         t, h, _ = vc.sync(clusters=False)
         n = plan[k][2] - plan[k][1]
         for buf, src, nbytes in ((o["atomics"], vc.out.atomics, 4 * (2 * n + 1)),
@@ -449,7 +452,7 @@ def run_e2e(args, chunks, plan, local_rank, torch, world, dist, threshold, weigh
     def step():
         pending = None
         for k, (ci, a, b) in enumerate(plan):
-            vc, s = ctxs[k % 2], streams[k % 2]
+            vc, s = ctxs[k % nctx], streams[k % nctx]
             base = int(chunks[ci].offsets[a])
             nbytes = int(chunks[ci].offsets[b]) - base
             sub = events.EventBatch(chunks[ci].raw[base:base + nbytes], offs[k])
@@ -484,7 +487,7 @@ def run_e2e(args, chunks, plan, local_rank, torch, world, dist, threshold, weigh
     n_events = sum(b - a for _, a, b in plan)
     return {"value": n_events * world * args.steps / el, "unit": UNIT,
             "h2d_bytes_per_step": h2d[0] // args.steps, "d2h_bytes_per_step": d2h[0] // args.steps,
-            "timing": "host wall clock around K steps, synchronised"}
+            "timing": "host wall clock around K steps, synchronised", "contexts": nctx}
 
 
 # ---------------------------------------------------------------------------
