@@ -246,12 +246,17 @@ __device__ __forceinline__ void store_state(char* base, uint32_t T, uint32_t i, 
 // taken 32 at a time, one per lane: an exclusive warp scan of their hit counts gives
 // their slices of the output; the hits of the 32 tracks form one contiguous range of the
 // Velo::Consolidated::Hits SoA, which the warp then writes in order (coalesced), each lane
-// finding the track of an output position by binary search over the 32 offsets. The fits
-// run per lane on the track's hits.
+// finding the track of an output position by binary search over the 32 offsets. The same
+// loop keeps x, y, z of the range in shared memory (up to kConsolidateStage hits), from
+// where the fits run per lane on their track's slice; a larger range (32 tracks averaging
+// more than 16 hits) fits from per-lane copies instead.
+constexpr uint32_t kConsolidateStage = 512;
+
 template<int WPB>
 __global__ void __launch_bounds__(WPB * 32) consolidate_fit_kernel(ChainPointers P)
 {
   __shared__ uint32_t s_off[WPB][33];
+  __shared__ float s_hit[WPB][3][kConsolidateStage];
   const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
   const uint32_t e = blockIdx.x * WPB + warp;
   if (e >= P.n_events) return;
@@ -283,6 +288,7 @@ __global__ void __launch_bounds__(WPB * 32) consolidate_fit_kernel(ChainPointers
     if (lane == 31) s_off[warp][32] = incl;
     __syncwarp();
     // coalesced write of the chunk's hit range [carry, carry + chunk_hits)
+    const bool staged = chunk_hits <= kConsolidateStage;
     for (uint32_t j = lane; j < chunk_hits; j += 32) {
       uint32_t lo = 0, hi = 32;  // last track with s_off <= j
       while (hi - lo > 1) {
@@ -295,20 +301,33 @@ __global__ void __launch_bounds__(WPB * 32) consolidate_fit_kernel(ChainPointers
       oy[carry + j] = p.y;
       oz[carry + j] = p.z;
       oid[carry + j] = ids[h];
+      if (staged) {
+        s_hit[warp][0][j] = p.x;
+        s_hit[warp][1][j] = p.y;
+        s_hit[warp][2][j] = p.z;
+      }
     }
+    __syncwarp();
     if (i < nt) {
       const uint32_t hoff = carry + s_off[warp][lane];
-      float hx[kMaxTrackSize], hy[kMaxTrackSize], hz[kMaxTrackSize];
-      for (uint32_t k = 0; k < n; ++k) {
-        const float4 p = H[track_hits[i * kMaxTrackSize + k]];
-        hx[k] = p.x;
-        hy[k] = p.y;
-        hz[k] = p.z;
-      }
       P.track_hit_number[t0 + i] = hoff;
-      const FitState beam = beamline_fit(hx, hy, hz, n);
+      FitState beam, kal;
+      if (staged) {
+        const uint32_t o = s_off[warp][lane];
+        beam = beamline_fit(&s_hit[warp][0][o], &s_hit[warp][1][o], &s_hit[warp][2][o], n);
+        kal = kalman_fit(&s_hit[warp][0][o], &s_hit[warp][1][o], &s_hit[warp][2][o], n, beam);
+      } else {
+        float hx[kMaxTrackSize], hy[kMaxTrackSize], hz[kMaxTrackSize];
+        for (uint32_t k = 0; k < n; ++k) {
+          const float4 p = H[track_hits[i * kMaxTrackSize + k]];
+          hx[k] = p.x;
+          hy[k] = p.y;
+          hz[k] = p.z;
+        }
+        beam = beamline_fit(hx, hy, hz, n);
+        kal = kalman_fit(hx, hy, hz, n, beam);
+      }
       store_state(P.states, T, t0 + i, beam);
-      const FitState kal = kalman_fit(hx, hy, hz, n, beam);
       store_state(P.kalman_states, T, t0 + i, kal);
     }
     carry += chunk_hits;
