@@ -6,8 +6,9 @@ and against the plain search it prunes.
   the deviation of the bf16 gradient from exact float64 maths is stated and bounded;
 * collected samples: features equal the oracle's restatement computed from the chain's own
   clusters, labels equal the plain search's tracks;
-* the pruned mode with nothing pruned (every event past the occupancy limit, or a scorer
-  that keeps everything) reproduces the plain chain exactly;
+* the pruned mode with nothing pruned (every event past the occupancy limit, a scorer
+  that keeps everything, or a scoring gate no candidate reaches) reproduces the plain chain
+  exactly, and seeds below the gate are kept unscored;
 * a trained scorer keeps long-track efficiency within 0.2% absolute of the plain search,
   does not raise the ghost rate, and makes the search explore fewer seeds and run faster.
 """
@@ -182,6 +183,37 @@ def test_pruned_without_pruning_is_plain():
     assert np.all((fb["status"] & chain.STATUS["mlp_fallback"]) != 0)
     for k in ("x", "y", "tx", "ty"):
         assert np.array_equal(fb["states"][k], plain["states"][k])
+
+
+def test_scoring_gate():
+    b = events.generate(seed=12, nu_min=2.0, nu_max=15.0, n_events=64, with_mc=False)
+    ref = canonical(run_mode(b, chain.MODE_PLAIN), b.n_events)
+    # a scorer that prunes every candidate it scores
+    d = random_weights(13, scale=0.0)
+    d["w3"][:, 64] = -30.0
+    d["seed_threshold"] = 0.5
+    # gate above every pair count: nothing is scored, every seed kept
+    d["min_pairs"] = 1 << 30
+    gated = run_mode(b, chain.MODE_PRUNED, mlp.dict_to_weights(d))
+    assert canonical(gated, b.n_events) == ref
+    # gate of 8 pairs: seeds kept exactly when their windows give fewer than 8 pairs
+    d["min_pairs"] = 8
+    res = run_mode(b, chain.MODE_PRUNED, mlp.dict_to_weights(d))
+    ms, mn = res["module_start"].reshape(-1, 52), res["module_num"].reshape(-1, 52)
+    n_small = n_large = 0
+    for e in range(b.n_events):
+        mods = chain.event_clusters(res, e)
+        cat = {k: np.concatenate([m[k] for m in mods]) for k in ("x", "y", "z", "phi", "size")}
+        idx, _, fo = mlp_oracle.event_features(cat["x"], cat["y"], cat["z"], cat["phi"], cat["size"],
+                                               [len(m["phi"]) for m in mods])
+        keep = res["cluster_keep"][ms[e, 0]:ms[e, 51] + mn[e, 51]]
+        pairs = fo[:, 6] * fo[:, 7]
+        small = pairs < 8
+        assert np.all(keep[idx[small]] & 1), e
+        assert not np.any(keep[idx[~small]] & 1), e
+        n_small += int(small.sum())
+        n_large += int((~small).sum())
+    assert n_small > 0 and n_large > 0
 
 
 def test_trained_scorer_prunes_at_no_efficiency_cost():
