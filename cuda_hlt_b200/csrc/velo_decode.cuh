@@ -377,7 +377,7 @@ __global__ void __launch_bounds__(W * 32) decode_cluster_sort_kernel(ChainPointe
     const bool event_ok = !(sh.flags & kStatusBadRawEvent);
     if (!event_ok)
       for (uint32_t b = threadIdx.x; b <= kSensors; b += blockDim.x) sh.sp_prefix[b] = 0;
-    // ---- bank prefix (warp 0) and sortedness of each bank ----
+    // ---- bank prefix (warp 0) ----
     if (event_ok) {
       if (warp == 0) {
         uint32_t carry = 0;
@@ -395,24 +395,26 @@ __global__ void __launch_bounds__(W * 32) decode_cluster_sort_kernel(ChainPointe
         }
         if (lane == 0) sh.sp_prefix[kSensors] = carry;
       }
-      for (uint32_t b = warp; b < kSensors; b += W) {
-        const uint32_t* bank = ev + sh.bank_start[b];
-        const uint32_t count = sh.bank_count[b];
-        bool unsorted = false;
-        for (uint32_t i = lane + 1; i < count; i += 32)
-          unsorted |= sp_addr(__ldg(bank + i)) < sp_addr(__ldg(bank + i - 1));
-        if (__any_sync(0xFFFFFFFFu, unsorted) && lane == 0) atomicOr(&sh.unsorted[b >> 5], 1u << (b & 31));
-      }
     }
     __syncthreads();
     const uint32_t total_sp = sh.sp_prefix[kSensors];
     const uint32_t base = static_cast<uint32_t>(off / 4);
     const bool use_map = event_ok && total_sp <= kBankMapCap;  // counts are valid only then
-    if (use_map) {
-      for (uint32_t b = warp; b < kSensors; b += W)
-        for (uint32_t i = lane; i < sh.bank_count[b]; i += 32) su.lists.bank_map[sh.sp_prefix[b] + i] = static_cast<uint8_t>(b);
-      __syncthreads();
+    // ---- bank of every SP (map) and sortedness of each bank, one pass over the flat SP
+    // index: every thread's loads are independent, so the first touches of the raw event
+    // overlap instead of queueing bank by bank ----
+    if (event_ok) {
+      for (uint32_t f = threadIdx.x; f < total_sp; f += blockDim.x) {
+        const uint32_t b = bank_of(sh, f);
+        if (use_map) su.lists.bank_map[f] = static_cast<uint8_t>(b);
+        const uint32_t s = f - sh.sp_prefix[b];
+        if (s > 0) {
+          const uint32_t* bank = ev + sh.bank_start[b];
+          if (sp_addr(__ldg(bank + s)) < sp_addr(__ldg(bank + s - 1))) atomicOr(&sh.unsorted[b >> 5], 1u << (b & 31));
+        }
+      }
     }
+    __syncthreads();
     const DecodeEvent d{ev, 2 * base, P.stage.xyzp, P.stage.id, use_map ? su.lists.bank_map : nullptr};
     // ---- pass 1: isolated SPs, candidate search of the others ----
     uint32_t my_cands = 0;
