@@ -159,6 +159,7 @@ __device__ __forceinline__ bool flood_window(uint32_t px0, uint32_t px1, uint32_
 
 constexpr uint32_t kCandCap = 4096;    // candidate pixels listed per event (more: flooded inline)
 constexpr uint32_t kBankMapCap = 16384; // SPs per event with a bank map (more: binary search)
+constexpr uint32_t kNonIsoCap = 2048;   // non-isolated SPs listed per event (more: full rescan)
 constexpr uint32_t kRegSortMax = 128;  // modules up to this size are sorted in registers
 
 struct DecodeShared {
@@ -173,6 +174,7 @@ struct DecodeShared {
   uint32_t flags;
   uint32_t n_candidates;
   uint32_t n_list;
+  uint32_t n_noniso;  // non-isolated SPs met by the first pass
 };
 
 __device__ __forceinline__ uint32_t bank_of(const DecodeShared& sh, uint32_t f)
@@ -314,8 +316,9 @@ __device__ __forceinline__ void warp_smem_sort(unsigned long long* key, uint32_t
   }
 }
 
+// 40 warps per SM (5 blocks of 8): 48 registers, no spills
 template<int W>
-__global__ void __launch_bounds__(W * 32) decode_cluster_sort_kernel(ChainPointers P)
+__global__ void __launch_bounds__(W * 32, 40 / W) decode_cluster_sort_kernel(ChainPointers P)
 {
   __shared__ DecodeShared sh;
   // the candidate list and the per-warp sort buffers are never live together
@@ -323,6 +326,7 @@ __global__ void __launch_bounds__(W * 32) decode_cluster_sort_kernel(ChainPointe
     struct {
       uint32_t cand[kCandCap];
       uint8_t bank_map[kBankMapCap];  // flat SP index -> bank, saves a binary search per SP
+      uint16_t noniso[kNonIsoCap];    // flat SP indices of the non-isolated SPs
     } lists;
     unsigned long long key[W][kSortCap];
   } su;
@@ -335,6 +339,7 @@ __global__ void __launch_bounds__(W * 32) decode_cluster_sort_kernel(ChainPointe
       sh.flags = 0;
       sh.n_candidates = 0;
       sh.n_list = 0;
+      sh.n_noniso = 0;
     }
     if (threadIdx.x < (kSensors + 31) / 32) sh.unsorted[threadIdx.x] = 0;
     if (threadIdx.x < kModules) sh.mod_count[threadIdx.x] = 0;
@@ -400,49 +405,59 @@ __global__ void __launch_bounds__(W * 32) decode_cluster_sort_kernel(ChainPointe
     const uint32_t total_sp = sh.sp_prefix[kSensors];
     const uint32_t base = static_cast<uint32_t>(off / 4);
     const bool use_map = event_ok && total_sp <= kBankMapCap;  // counts are valid only then
-    // ---- bank of every SP (map) and sortedness of each bank, one pass over the flat SP
-    // index: every thread's loads are independent, so the first touches of the raw event
-    // overlap instead of queueing bank by bank ----
+    const DecodeEvent d{ev, 2 * base, P.stage.xyzp, P.stage.id, use_map ? su.lists.bank_map : nullptr};
+    // ---- pass 1, one pass over the flat SP index: bank of every SP (map), sortedness of each
+    // bank, and the clusters of the isolated SPs from the pattern table (they need neither);
+    // the non-isolated SPs are listed for pass 2. Every thread's loads are independent, so
+    // the first touches of the raw event overlap instead of queueing bank by bank ----
+    const bool can_list = total_sp <= 0x10000u;  // list entries are 16-bit
     if (event_ok) {
       for (uint32_t f = threadIdx.x; f < total_sp; f += blockDim.x) {
         const uint32_t b = bank_of(sh, f);
         if (use_map) su.lists.bank_map[f] = static_cast<uint8_t>(b);
         const uint32_t s = f - sh.sp_prefix[b];
-        if (s > 0) {
-          const uint32_t* bank = ev + sh.bank_start[b];
-          if (sp_addr(__ldg(bank + s)) < sp_addr(__ldg(bank + s - 1))) atomicOr(&sh.unsorted[b >> 5], 1u << (b & 31));
+        const uint32_t* bank = ev + sh.bank_start[b];
+        const uint32_t word = __ldg(bank + s);
+        if (s > 0 && sp_addr(word) < sp_addr(__ldg(bank + s - 1))) atomicOr(&sh.unsorted[b >> 5], 1u << (b & 31));
+        if (sp_isolated(word)) {
+          // pattern table (MaskedVeloClustering.cu:105-167)
+          const uint32_t sp = sp_mask(word);
+          const int32_t sp_r = sp_row(word), sp_c = sp_col(word);
+          const uint32_t idx = __ldg(P.k.sp_patterns + sp);
+          const uint32_t chip = sp_c / (kChipColumns / 2);
+          const uint32_t sensor = sh.bank_sensor[b];
+          for (int c = 0; c < 2; ++c) {
+            if (c == 1 && !(idx & 8)) break;
+            const uint32_t row = c ? (idx >> 4) & 3u : idx & 0x03u;
+            const uint32_t col = c ? (idx >> 6) & 1u : (idx >> 2) & 1u;
+            const uint32_t cx = sp_c * 2 + col;
+            const uint32_t cy = sp_r * 4 + row;
+            const float fx = __ldg(P.k.sp_fx + sp * 2 + c);
+            const float fy = __ldg(P.k.sp_fy + sp * 2 + c);
+            stage_cluster(sh, d, b >> 2, place_cluster(g, sensor, cx, cy, fx, fy, chip),
+                          (__ldg(P.k.sp_sizes + sp) >> (4 * c)) & 0xFu);
+          }
+        } else if (can_list) {
+          const uint32_t q = atomicAdd(&sh.n_noniso, 1u);
+          if (q < kNonIsoCap) su.lists.noniso[q] = static_cast<uint16_t>(f);
         }
       }
     }
     __syncthreads();
-    const DecodeEvent d{ev, 2 * base, P.stage.xyzp, P.stage.id, use_map ? su.lists.bank_map : nullptr};
-    // ---- pass 1: isolated SPs, candidate search of the others ----
+    // ---- pass 2: candidate search of the non-isolated SPs (from the list, or every SP when
+    // the list overflowed) ----
     uint32_t my_cands = 0;
-    for (uint32_t f = threadIdx.x; f < total_sp; f += blockDim.x) {
+    const bool listed = can_list && sh.n_noniso <= kNonIsoCap;
+    const uint32_t n_scan = listed ? sh.n_noniso : total_sp;
+    for (uint32_t i = threadIdx.x; i < n_scan; i += blockDim.x) {
+      const uint32_t f = listed ? su.lists.noniso[i] : i;
       const uint32_t b = bank_of_sp(sh, d, f);
       const uint32_t s = f - sh.sp_prefix[b];
       const uint32_t* bank = ev + sh.bank_start[b];
       const uint32_t word = __ldg(bank + s);
+      if (sp_isolated(word)) continue;  // emitted in pass 1
       const uint32_t sp = sp_mask(word);
       const int32_t sp_r = sp_row(word), sp_c = sp_col(word);
-      if (sp_isolated(word)) {
-        // pattern table (MaskedVeloClustering.cu:105-167)
-        const uint32_t idx = __ldg(P.k.sp_patterns + sp);
-        const uint32_t chip = sp_c / (kChipColumns / 2);
-        const uint32_t sensor = sh.bank_sensor[b];
-        for (int c = 0; c < 2; ++c) {
-          if (c == 1 && !(idx & 8)) break;
-          const uint32_t row = c ? (idx >> 4) & 3u : idx & 0x03u;
-          const uint32_t col = c ? (idx >> 6) & 1u : (idx >> 2) & 1u;
-          const uint32_t cx = sp_c * 2 + col;
-          const uint32_t cy = sp_r * 4 + row;
-          const float fx = __ldg(P.k.sp_fx + sp * 2 + c);
-          const float fy = __ldg(P.k.sp_fy + sp * 2 + c);
-          stage_cluster(sh, d, b >> 2, place_cluster(g, sensor, cx, cy, fx, fy, chip),
-                        (__ldg(P.k.sp_sizes + sp) >> (4 * c)) & 0xFu);
-        }
-        continue;
-      }
       const bool sorted = !((sh.unsorted[b >> 5] >> (b & 31)) & 1u);
       const uint32_t code = window_candidate_code(sp, gather_window(bank, sh.bank_count[b], sorted, sp_r, sp_c));
       for (int half = 0; half < 2; ++half) {
@@ -459,7 +474,7 @@ __global__ void __launch_bounds__(W * 32) decode_cluster_sort_kernel(ChainPointe
     for (int o = 16; o > 0; o >>= 1) my_cands += __shfl_xor_sync(0xFFFFFFFFu, my_cands, o);
     if (lane == 0 && my_cands) atomicAdd(&sh.n_candidates, my_cands);
     __syncthreads();
-    // ---- pass 2: flood fill of the listed candidates ----
+    // ---- pass 3: flood fill of the listed candidates ----
     const uint32_t n_list = min(sh.n_list, kCandCap);
     for (uint32_t i = threadIdx.x; i < n_list; i += blockDim.x) {
       const uint32_t c = su.lists.cand[i];
