@@ -107,6 +107,11 @@ HOST_SYMBOLS = [
     "velo_gen_copy",
     "velo_gen_destroy",
     "velo_check_tracks",
+    "velo_mdf_read",
+    "velo_mdf_count",
+    "velo_mdf_raw_bytes",
+    "velo_mdf_copy",
+    "velo_mdf_free",
 ]
 GPU_SYMBOLS = [
     "velo_create",
@@ -165,6 +170,16 @@ def host_lib():
         lib.velo_gen_destroy.restype = None
         lib.velo_check_tracks.argtypes = [P, P, C.c_uint32, P, P, P, C.POINTER(VeloCheckResult)]
         lib.velo_check_tracks.restype = C.c_int
+        lib.velo_mdf_read.argtypes = [C.c_char_p, C.c_uint64, C.c_uint64, C.POINTER(P)]
+        lib.velo_mdf_read.restype = C.c_int
+        lib.velo_mdf_count.argtypes = [P]
+        lib.velo_mdf_count.restype = C.c_uint64
+        lib.velo_mdf_raw_bytes.argtypes = [P]
+        lib.velo_mdf_raw_bytes.restype = C.c_uint64
+        lib.velo_mdf_copy.argtypes = [P, P, P, P, P]
+        lib.velo_mdf_copy.restype = C.c_int
+        lib.velo_mdf_free.argtypes = [P]
+        lib.velo_mdf_free.restype = None
         _host = lib
     return _host
 

@@ -1,6 +1,6 @@
 """Builds the in-tree shared libraries of the package.
 
-  libvelo_host.so  host utilities (g++)
+  libvelo_host.so  host utilities: generator, MC checker, MDF reader (g++, zlib)
   libvelo_b200.so  sm_100a kernels + C-ABI context (nvcc), linked against libvelo_host.so
 
 The kernels are compiled with --use_fast_math, the math mode of the stage they replace
@@ -39,10 +39,11 @@ def _sources(ext):
 
 def build_host(force=False):
     lib = os.path.join(HERE, "libvelo_host.so")
-    srcs = [os.path.join(CSRC, "velo_host.cpp")]
+    srcs = [os.path.join(CSRC, "velo_host.cpp"), os.path.join(CSRC, "velo_mdf.cpp")]
     deps = srcs + _sources(".hpp") + [os.path.join(INCLUDE, "velo_b200.h")]
     if force or _newer(lib, deps):
-        sh(["g++", "-O3", "-std=c++17", "-fPIC", "-shared", "-Wall", f"-I{INCLUDE}", "-o", lib] + srcs + ["-lpthread"])
+        sh(["g++", "-O3", "-std=c++17", "-fPIC", "-shared", "-Wall", f"-I{INCLUDE}", "-o", lib] + srcs +
+           ["-lpthread", "-lz"])
     return lib
 
 

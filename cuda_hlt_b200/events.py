@@ -121,6 +121,40 @@ def read_bank_folder(vp_folder, mc_folder=None, limit=None):
     return batch
 
 
+def read_mdf(path, first_event=0, max_events=None):
+    """VP raw banks of the events of an MDF file (velo_mdf_read, the counterpart of
+    MDF::read_events for BankTypes::VP) or of every *.mdf file of a folder in name order;
+    event names are "run_event" from the ODIN bank."""
+    import ctypes as C
+    lib = _lib.host_lib()
+    files = sorted(glob.glob(os.path.join(path, "*.mdf"))) if os.path.isdir(path) else [path]
+    raws, names, skip = [], [], first_event
+    left = (1 << 62) if max_events is None else max_events
+    for f in files:
+        h = C.c_void_p()
+        rc = lib.velo_mdf_read(f.encode(), skip, left, C.byref(h))
+        if rc != 0:
+            raise ValueError(f"velo_mdf_read({f}) failed with code {rc}")
+        try:
+            n = lib.velo_mdf_count(h)
+            raw = np.zeros(lib.velo_mdf_raw_bytes(h), np.uint8)
+            off = np.zeros(n + 1, np.uint64)
+            run = np.zeros(n, np.uint32)
+            evn = np.zeros(n, np.uint64)
+            lib.velo_mdf_copy(h, raw.ctypes.data, off.ctypes.data, run.ctypes.data, evn.ctypes.data)
+        finally:
+            lib.velo_mdf_free(h)
+        raws += [raw[off[i]:off[i + 1]] for i in range(n)]
+        names += [f"{run[i]}_{evn[i]}" for i in range(n)]
+        left -= n
+        skip = 0  # counted in the first file only
+        if left <= 0:
+            break
+    offsets = np.zeros(len(raws) + 1, dtype=np.uint64)
+    offsets[1:] = np.cumsum([r.size for r in raws])
+    return EventBatch(np.concatenate(raws) if raws else np.zeros(0, np.uint8), offsets, names=names)
+
+
 def validate(batch):
     """Per-event raw-format check; returns a bool array (True = well formed)."""
     lib = _lib.host_lib()

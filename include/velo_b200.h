@@ -117,6 +117,22 @@ int velo_check_tracks(const void* mc_blob, const uint64_t* mc_offsets, uint32_t 
                       const uint32_t* event_track_offsets, const uint32_t* track_hit_offsets, const uint32_t* hit_ids,
                       VeloCheckResult* res);
 
+/* MDF reader: the VP raw banks of the events of an LHCb MDF file in the raw layout velo_run
+ * takes (number of banks, byte offsets, per bank its source id and body), with the ODIN run
+ * and event number of each event. Replaces MDF::read_events (mdf/src/read_mdf.cpp:29-191,
+ * driven by MDFReader::read_events, main/src/MDFReader.cpp:15-63) for BankTypes::VP on one
+ * file: skips `first_event` events, then reads up to `max_events`. zlib-compressed records
+ * (ROOT blocks) are expanded and record checksums verified. Errors: VELO_ERR_INVALID (no
+ * file), VELO_ERR_BAD_RAW (bad header, checksum, compressed block or raw bank; the
+ * reference prints and stops at the first such record, or, for a bad bank magic, goes on). */
+typedef struct VeloMdfEvents VeloMdfEvents;
+int velo_mdf_read(const char* path, uint64_t first_event, uint64_t max_events, VeloMdfEvents** out);
+uint64_t velo_mdf_count(const VeloMdfEvents* events);
+uint64_t velo_mdf_raw_bytes(const VeloMdfEvents* events);
+/* raw[raw_bytes], offsets[count + 1] (u64 byte offsets), run[count], event[count]; any may be null */
+int velo_mdf_copy(const VeloMdfEvents* events, void* raw, uint64_t* offsets, uint32_t* run, uint64_t* event);
+void velo_mdf_free(VeloMdfEvents* events);
+
 /* ======================================================================
  * GPU chain (libvelo_b200.so)
  * ====================================================================== */

@@ -1,8 +1,9 @@
 """Generates the committed fixtures under tests/golden/.
 
-  minbias/VP/*.bin, minbias/MC_tracks/*.bin
-      the 10 real minbias events shipped with the reference (input/minbias/banks/VP and
-      input/minbias/MC_info/tracks), copied as data: raw VP banks and their MC truth.
+  minbias/VP/*.bin, minbias/MC_tracks/*.bin, minbias/mdf/*.mdf
+      the 10 real minbias events shipped with the reference (input/minbias/banks/VP,
+      input/minbias/MC_info/tracks and input/minbias/banks/mdf), copied as data: raw VP
+      banks, their MC truth, and the same events as an MDF file (all banks, compressed).
   ref_gpu_*.npz
       outputs of the reference's own CUDA kernels (oracle/_ref/libvelo_ref_gpu.so) on the
       minbias events and on seeded synthetic events; written by `--ref-gpu` on a GPU box
@@ -21,7 +22,7 @@ REF = "/root/reference"
 
 
 def copy_minbias():
-    for sub, dst in (("banks/VP", "VP"), ("MC_info/tracks", "MC_tracks")):
+    for sub, dst in (("banks/VP", "VP"), ("MC_info/tracks", "MC_tracks"), ("banks/mdf", "mdf")):
         src = os.path.join(REF, "input/minbias", sub)
         out = os.path.join(HERE, "minbias", dst)
         os.makedirs(out, exist_ok=True)
