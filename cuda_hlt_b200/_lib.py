@@ -93,6 +93,10 @@ class VeloOutputs(C.Structure):
         ("hit_capacity", C.c_uint64),
         ("hit_size", C.c_void_p),
         ("hit_keep", C.c_void_p),
+        ("pv_vertices", C.c_void_p),
+        ("pv_count", C.c_void_p),
+        ("pv_zpeaks", C.c_void_p),
+        ("pv_npeaks", C.c_void_p),
     ]
 
 
@@ -129,6 +133,7 @@ GPU_SYMBOLS = [
     "velo_search_static",
     "velo_version",
     "velo_set_mode",
+    "velo_set_pv",
     "velo_mlp_trainer_create",
     "velo_mlp_trainer_destroy",
     "velo_mlp_collect",
@@ -222,6 +227,8 @@ def gpu_lib():
         lib.velo_version.restype = C.c_char_p
         lib.velo_set_mode.argtypes = [P, C.c_uint32]
         lib.velo_set_mode.restype = C.c_int
+        lib.velo_set_pv.argtypes = [P, C.c_int]
+        lib.velo_set_pv.restype = C.c_int
         W = C.POINTER(VeloMlpWeights)
         lib.velo_mlp_trainer_create.argtypes = [C.c_int, C.c_uint64, C.c_uint64, C.POINTER(P)]
         lib.velo_mlp_trainer_destroy.argtypes = [P]

@@ -31,7 +31,12 @@ SEQUENCE = (
     "velo_kalman_fit_t",
 )
 
-STAGES = ("decode_cluster_sort", "fill_candidates", "search_by_triplet", "event_scan", "consolidate_fit")
+STAGES = ("decode_cluster_sort", "fill_candidates", "search_by_triplet", "event_scan", "consolidate_fit", "pv_beamline")
+PV_MAX_VERTICES = 32
+# VeloPvVertex (PV::Vertex layout)
+PV_VERTEX = np.dtype([("x", "<f4"), ("y", "<f4"), ("z", "<f4"), ("chi2", "<f4"), ("ndof", "<i4"), ("n_tracks", "<u4"),
+                      ("cov00", "<f4"), ("cov10", "<f4"), ("cov11", "<f4"), ("cov20", "<f4"), ("cov21", "<f4"),
+                      ("cov22", "<f4"), ("n_tracks_unused", "<i4")])
 MODE_PLAIN, MODE_PRUNED = 0, 1
 MAP_AUTO, MAP_BLOCK, MAP_WARP = 0, 1, 2
 N_MODULES = 52
@@ -125,6 +130,10 @@ class VeloChain:
         out["runs"] = int(ms[n])
         return out
 
+    def set_pv(self, enabled=True):
+        """Appends the beamline primary-vertex finder to every run (velo_set_pv)."""
+        _check(self.lib.velo_set_pv(self.ctx, int(bool(enabled))), "velo_set_pv")
+
     def set_mode(self, mode):
         """MODE_PLAIN (reference semantics) or MODE_PRUNED (learned scorer, set_mlp first)."""
         _check(self.lib.velo_set_mode(self.ctx, int(mode)), "velo_set_mode")
@@ -159,13 +168,20 @@ class VeloChain:
         thn = self._down(o.track_hit_number, np.uint32, T + 1)
         H = int(thn[T]) if T else 0
         hits = self._down(o.track_hits, np.uint8, 16 * H)
+        kalman_raw = self._down(o.kalman_states, np.uint8, 52 * T)
         hv = hits.view(np.float32).reshape(4, H) if H else np.zeros((4, 0), np.float32)
         res = dict(
             atomics=atomics, n_tracks=atomics[:N], track_offsets=atomics[N:2 * N + 1], track_hit_number=thn,
             hit_x=hv[0], hit_y=hv[1], hit_z=hv[2], hit_id=hv[3].view(np.uint32),
             states=decode_states(self._down(o.states, np.uint8, 52 * T).tobytes(), T),
-            kalman=decode_states(self._down(o.kalman_states, np.uint8, 52 * T).tobytes(), T),
+            kalman=decode_states(kalman_raw.tobytes(), T), kalman_raw=kalman_raw,
             status=self._down(o.status, np.uint32, N))
+        if o.pv_vertices:
+            M = PV_MAX_VERTICES
+            res["pv_vertices"] = self._down(o.pv_vertices, np.uint8, N * M * PV_VERTEX.itemsize).view(PV_VERTEX).reshape(N, M)
+            res["pv_count"] = self._down(o.pv_count, np.uint32, N)
+            res["pv_zpeaks"] = self._down(o.pv_zpeaks, np.float32, N * M).reshape(N, M)
+            res["pv_npeaks"] = self._down(o.pv_npeaks, np.uint32, N)
         if clusters:
             res["module_start"] = self._down(o.module_hit_start, np.uint32, N * N_MODULES)
             res["module_num"] = self._down(o.module_hit_num, np.uint32, N * N_MODULES)

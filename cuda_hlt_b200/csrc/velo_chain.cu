@@ -19,6 +19,7 @@
 #include "velo_search.cuh"
 #include "velo_search_block.cuh"
 #include "velo_consolidate.cuh"
+#include "velo_pv.cuh"
 
 // ============================================================================
 // C-ABI context
@@ -66,6 +67,12 @@ struct VeloCtx {
   uint32_t* d_queue = nullptr;
   uint32_t *d_warp_events = nullptr, *d_block_events = nullptr, *d_event_order = nullptr;
   uint32_t block_threshold = 0;  // clusters above which an event takes the block search
+  // beamline PV stage (velo_set_pv)
+  bool pv = false;
+  PvTrack* d_pv_tracks = nullptr;
+  PvVertex* d_pv_vertices = nullptr;
+  uint32_t *d_pv_count = nullptr, *d_pv_npeaks = nullptr;
+  float* d_pv_zpeaks = nullptr;
   uint32_t* h_totals = nullptr;  // pinned [4]
   cudaStream_t last_stream = nullptr;
   uint32_t last_n = 0;
@@ -73,7 +80,7 @@ struct VeloCtx {
   bool timing = false;
   // Stage timing: one set of kStageEvents events per launch sequence; a graph keeps the set
   // it was captured with, plain launches cycle through the sets.
-  static constexpr int kStageEvents = 6;
+  static constexpr int kStageEvents = 7;
   std::vector<std::array<cudaEvent_t, kStageEvents>> ev_sets;
   std::vector<uint8_t> ev_used;
   uint32_t ev_next = 0;
@@ -131,7 +138,8 @@ void free_all(VeloCtx* c)
                   c->d_event_hits, c->d_status, c->d_track_n, c->d_track_hits, c->d_tracklets, c->d_weak, c->d_ttf,
                   c->d_event_tracks, c->d_event_track_hits, c->d_atomics, c->d_track_hit_number,
                   c->d_event_hit_offset, c->d_track_hits_out, c->d_states, c->d_kalman, c->d_queue,
-                  c->d_warp_events, c->d_block_events, c->d_event_order};
+                  c->d_warp_events, c->d_block_events, c->d_event_order, c->d_pv_tracks, c->d_pv_vertices,
+                  c->d_pv_count, c->d_pv_npeaks, c->d_pv_zpeaks};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c->h_totals) cudaFreeHost(c->h_totals);
@@ -255,6 +263,13 @@ int launch_chain(VeloCtx* c, const ChainPointers& P, cudaStream_t s, bool captur
   VCK(cudaGetLastError());
   ++c->launches;
   if (c->timing && c->ev_current >= 0) VCK(record(c->ev_sets[c->ev_current][5], s, capturing));
+  if (c->pv) {
+    const PvPointers V{c->d_kalman, c->d_pv_tracks, c->d_pv_vertices, c->d_pv_count, c->d_pv_zpeaks, c->d_pv_npeaks};
+    pv_beamline_kernel<<<n, kPvThreads, 0, s>>>(P, V);
+    VCK(cudaGetLastError());
+    ++c->launches;
+  }
+  if (c->timing && c->ev_current >= 0) VCK(record(c->ev_sets[c->ev_current][6], s, capturing));
   return 0;
 }
 
@@ -331,6 +346,11 @@ int velo_create(const VeloConfig* cfg, const void* geometry, size_t geometry_byt
   ok &= dalloc(c->d_track_hits_out, 16 * TH) == cudaSuccess;
   ok &= dalloc(c->d_states, 52 * T) == cudaSuccess;
   ok &= dalloc(c->d_kalman, 52 * T) == cudaSuccess;
+  ok &= dalloc(c->d_pv_tracks, T) == cudaSuccess;
+  ok &= dalloc(c->d_pv_vertices, static_cast<size_t>(N) * kPvMaxVertices) == cudaSuccess;
+  ok &= dalloc(c->d_pv_zpeaks, static_cast<size_t>(N) * kPvMaxVertices) == cudaSuccess;
+  ok &= dalloc(c->d_pv_count, N) == cudaSuccess;
+  ok &= dalloc(c->d_pv_npeaks, N) == cudaSuccess;
   ok &= dalloc(c->d_queue, 8) == cudaSuccess;
   ok &= dalloc(c->d_warp_events, N) == cudaSuccess;
   ok &= dalloc(c->d_block_events, N) == cudaSuccess;
@@ -397,6 +417,12 @@ static int fill_outputs(VeloCtx* c, uint32_t n, VeloOutputs* out)
   out->hit_capacity = c->hit_capacity;
   out->hit_size = c->d_hit_size;
   out->hit_keep = c->mode == VELO_MODE_PRUNED ? c->d_keep : nullptr;
+  if (c->pv) {
+    out->pv_vertices = c->d_pv_vertices;
+    out->pv_count = c->d_pv_count;
+    out->pv_zpeaks = c->d_pv_zpeaks;
+    out->pv_npeaks = c->d_pv_npeaks;
+  }
   return 0;
 }
 
@@ -550,6 +576,14 @@ int velo_set_mode(VeloCtx* c, uint32_t mode)
   return 0;
 }
 
+int velo_set_pv(VeloCtx* c, int enabled)
+{
+  if (!c) return VELO_ERR_INVALID;
+  if ((enabled != 0) != c->pv) drop_graphs(c);  // the launch sequence changes
+  c->pv = enabled != 0;
+  return 0;
+}
+
 int velo_set_timing(VeloCtx* c, int enabled)
 {
   if (!c) return VELO_ERR_INVALID;
@@ -563,8 +597,9 @@ int velo_set_timing(VeloCtx* c, int enabled)
   return 0;
 }
 
-// Sums, over every event set recorded since velo_set_timing, the device time of the five
-// stages; ms[5] (when n > 5) receives the number of launch sequences summed.
+// Sums, over every event set recorded since velo_set_timing, the device time of the six
+// stages (the last, the PV stage, is 0 when it is off); ms[6] (when n > 6) receives the
+// number of launch sequences summed.
 int velo_stage_times(VeloCtx* c, float* ms, int n)
 {
   constexpr int kStages = VeloCtx::kStageEvents - 1;

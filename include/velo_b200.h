@@ -61,6 +61,8 @@ extern "C" {
 #define VELO_STATUS_H1_OVERFLOW (1u << 7)
 #define VELO_STATUS_BIG_SP_INDEX (1u << 8)
 #define VELO_STATUS_MLP_FALLBACK (1u << 9)
+#define VELO_STATUS_PV_OVERFLOW (1u << 13) /* PV stage: peaks, clusters or extrema beyond the
+                                              reference's fixed arrays (it writes past them) */
 
 /* ======================================================================
  * Host utilities (libvelo_host.so; no GPU needed)
@@ -183,7 +185,23 @@ typedef struct VeloOutputs {
   uint64_t hit_capacity;
   uint8_t* hit_size;
   uint8_t* hit_keep;
+  /* beamline PV stage (velo_set_pv; null when off) */
+  void* pv_vertices;     /* VeloPvVertex[n_events * VELO_PV_MAX_VERTICES], per event in seed order */
+  uint32_t* pv_count;    /* [n_events] vertices of each event */
+  float* pv_zpeaks;      /* [n_events * VELO_PV_MAX_VERTICES] z of the histogram peaks (seeds) */
+  uint32_t* pv_npeaks;   /* [n_events] */
 } VeloOutputs;
+
+/* A primary vertex, in the layout of PV::Vertex (cuda/PV/beamlinePV/include/PV_Definitions.cuh:64-109). */
+#define VELO_PV_MAX_VERTICES 32
+typedef struct VeloPvVertex {
+  float x, y, z;
+  float chi2;
+  int32_t ndof;      /* left unset by the reference; 0 */
+  uint32_t n_tracks; /* as the reference counts them: every track of the event */
+  float cov00, cov10, cov11, cov20, cov21, cov22;
+  int32_t n_tracks_unused;
+} VeloPvVertex;
 
 /* Creates a context: device buffers for cfg->max_events events, device constants from the
  * 19456-byte geometry blob (cuda/velo/common/src/ClusteringDefinitions.cu:23-53). */
@@ -262,7 +280,8 @@ int velo_mlp_infer(VeloMlpTrainer* t, const float* features, uint32_t n, float* 
 
 /* Device time of each stage of the runs recorded since velo_set_timing, milliseconds:
  * ms[0] decode+cluster+sort, ms[1] fill_candidates (windows, scorer), ms[2] search,
- * ms[3] scan, ms[4] consolidate+fit, ms[5] (n > 5) number of runs summed. */
+ * ms[3] scan, ms[4] consolidate+fit, ms[5] beamline PV (0 when off), ms[6] (n > 6) number of
+ * runs summed. */
 int velo_stage_times(VeloCtx* ctx, float* ms, int n);
 int velo_set_timing(VeloCtx* ctx, int enabled);
 
@@ -273,6 +292,12 @@ int velo_destroy(VeloCtx* ctx);
 int velo_download(VeloCtx* ctx, void* dst_host, const void* src_device, size_t bytes);
 /* Asynchronous variant on `stream` (dst_host should be pinned). */
 int velo_download_async(VeloCtx* ctx, void* dst_host, const void* src_device, size_t bytes, void* stream);
+
+/* Appends the beamline primary-vertex finder (cuda/PV/beamlinePV: pv_beamline_extrapolate,
+ * pv_beamline_histo, pv_beamline_peak, pv_beamline_multi_fitter of DefaultSequence.h:20-23)
+ * to every run, on the Kalman beamline states; its outputs are VeloOutputs.pv_*. Off by
+ * default. */
+int velo_set_pv(VeloCtx* ctx, int enabled);
 
 /* Search mapping: events with more than `clusters` clusters run the block-per-event search,
  * the others the warp-per-event search (0: all block, >= 16384: all warp). Set by the

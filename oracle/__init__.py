@@ -151,6 +151,9 @@ def ref_gpu_lib():
         L.ref_velo_run.restype = C.c_int
         L.ref_free.argtypes = [C.POINTER(RefOutputs)]
         L.ref_state_size.restype = C.c_int
+        L.ref_pv_vertex_size.restype = C.c_int
+        L.ref_pv_run.argtypes = [P, P, P, C.c_uint32, P, P, P, P, P]
+        L.ref_pv_run.restype = C.c_int
         _ref_gpu = L
     return _ref_gpu
 
@@ -193,6 +196,32 @@ def ref_gpu_run(batch, geometry, reps=1):
         return res, ms.value
     finally:
         L.ref_free(C.byref(out))
+
+
+REF_PV_NBINS, REF_PV_MAX_VERTICES = 2400, 32
+
+
+def ref_pv_run(atomics, track_hit_number, kalman_raw, n_events):
+    """The reference's beamline PV kernels (cuda/PV/beamlinePV) on consolidated VELO tracks:
+    atomics[2N+1], track_hit_number[T+1], Kalman states as raw bytes (sizeof(VeloState) * T).
+    Returns dict zhisto [N, 2400], zpeaks [N, 32], n_peaks [N], vertices (raw bytes,
+    PV::Vertex [N, 32]), n_vertices [N]."""
+    L = ref_gpu_lib()
+    N = int(n_events)
+    a = np.ascontiguousarray(atomics, np.uint32)
+    thn = np.ascontiguousarray(track_hit_number, np.uint32)
+    kal = np.ascontiguousarray(kalman_raw, np.uint8)
+    vs = L.ref_pv_vertex_size()
+    out = dict(zhisto=np.zeros((N, REF_PV_NBINS), np.float32), zpeaks=np.zeros((N, REF_PV_MAX_VERTICES), np.float32),
+               n_peaks=np.zeros(N, np.uint32), vertices=np.zeros(N * REF_PV_MAX_VERTICES * vs, np.uint8),
+               n_vertices=np.zeros(N, np.uint32))
+    rc = L.ref_pv_run(a.ctypes.data, thn.ctypes.data, kal.ctypes.data, N, out["zhisto"].ctypes.data,
+                      out["zpeaks"].ctypes.data, out["n_peaks"].ctypes.data, out["vertices"].ctypes.data,
+                      out["n_vertices"].ctypes.data)
+    if rc != 0:
+        raise RuntimeError(f"ref_pv_run failed: {rc}")
+    out["vertex_size"] = vs
+    return out
 
 
 def ref_event_clusters(res, e):

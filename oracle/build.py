@@ -54,7 +54,8 @@ def ref_includes():
             "cuda/utils/sorting/include", "cuda/utils/prefix_sum/include", "cuda/utils/binary_search/include",
             "main/include", "stream/gear/include", "stream/setup/include", "cuda/event_model/UT/include",
             "cuda/event_model/SciFi/include", "cuda/UT/PrVeloUT/include", "cuda/UT/common/include",
-            "cuda/SciFi/common/include", "cuda/SciFi/PrForward/include", "x86/velo/clustering/include"]
+            "cuda/SciFi/common/include", "cuda/SciFi/PrForward/include", "x86/velo/clustering/include",
+            "cuda/PV/beamlinePV/include", "cuda/PV/common/include", "cuda/utils/float_operations/include"]
     return [f"-I{os.path.join(REF, d)}" for d in dirs]
 
 
@@ -79,7 +80,7 @@ def build_ref_x86():
 def build_ref_gpu():
     kernel_dirs = ["cuda/velo/common/src", "cuda/velo/mask_clustering/src", "cuda/velo/calculate_phi_and_sort/src",
                    "cuda/velo/search_by_triplet/src", "cuda/velo/consolidate_tracks/src",
-                   "cuda/velo/simplified_kalman_filter/src", "cuda/utils/prefix_sum/src"]
+                   "cuda/velo/simplified_kalman_filter/src", "cuda/utils/prefix_sum/src", "cuda/PV/beamlinePV/src"]
     srcs = []
     for d in kernel_dirs:
         p = os.path.join(REF, d)

@@ -29,6 +29,10 @@
 #include "SearchByTriplet.cuh"
 #include "VeloKalmanFilter.cuh"
 #include "WeakTracksAdder.cuh"
+#include "pv_beamline_extrapolate.cuh"
+#include "pv_beamline_histo.cuh"
+#include "pv_beamline_multi_fitter.cuh"
+#include "pv_beamline_peak.cuh"
 
 namespace {
 
@@ -318,4 +322,55 @@ int ref_velo_run(const void* raw, const uint32_t* offsets, uint32_t n_events, co
 }
 
 int ref_state_size(void) { return static_cast<int>(sizeof(VeloState)); }
+int ref_pv_vertex_size(void) { return static_cast<int>(sizeof(PV::Vertex)); }
+
+// The reference's beamline PV finder (cuda/PV/beamlinePV: pv_beamline_extrapolate_t,
+// pv_beamline_histo_t, pv_beamline_peak_t, pv_beamline_multi_fitter_t of
+// DefaultSequence.h:20-23) on consolidated VELO tracks: atomics[2N+1], track_hit_number[T+1]
+// and Kalman beamline states (sizeof(VeloState) * T bytes, the States SoA). Launch shapes
+// and the vertex-count memset of stream/visitors/beamlinePV/src/*.cu. Outputs: the z
+// histograms [N * Nbins], peaks [N * 32] with counts [N], vertices [N * 32] with counts [N].
+int ref_pv_run(const uint32_t* atomics, const uint32_t* track_hit_number, const void* kalman, uint32_t n_events,
+               float* zhisto, float* zpeaks, uint32_t* n_peaks, void* vertices, uint32_t* n_vertices)
+{
+  if (!atomics || !track_hit_number || !kalman || n_events == 0) return -1;
+  const uint32_t N = n_events, T = atomics[2 * N];
+  cudaStream_t s;
+  CK(cudaStreamCreate(&s));
+  Buf d_atomics, d_hn, d_kal, d_trk, d_histo, d_peaks, d_npeaks, d_vtx, d_nvtx;
+  CK(d_atomics.ensure(4ull * (2 * N + 1)));
+  CK(d_hn.ensure(4ull * (T + 1)));
+  CK(d_kal.ensure(sizeof(VeloState) * (T > 0 ? T : 1)));
+  CK(d_trk.ensure(sizeof(PVTrack) * (T > 0 ? T : 1)));
+  CK(d_histo.ensure(4ull * N * Nbins));
+  CK(d_peaks.ensure(4ull * N * PV::max_number_vertices));
+  CK(d_npeaks.ensure(4ull * N));
+  CK(d_vtx.ensure(sizeof(PV::Vertex) * N * PV::max_number_vertices));
+  CK(d_nvtx.ensure(4ull * N));
+  CK(cudaMemcpy(d_atomics.p, atomics, 4ull * (2 * N + 1), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d_hn.p, track_hit_number, 4ull * (T + 1), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d_kal.p, kalman, sizeof(VeloState) * T, cudaMemcpyHostToDevice));
+  pv_beamline_extrapolate<<<dim3(N), dim3(128), 0, s>>>(static_cast<char*>(d_kal.p), static_cast<int*>(d_atomics.p),
+                                                        static_cast<uint*>(d_hn.p), static_cast<PVTrack*>(d_trk.p));
+  pv_beamline_histo<<<dim3(N), dim3(128), 0, s>>>(static_cast<int*>(d_atomics.p), static_cast<uint*>(d_hn.p),
+                                                  static_cast<PVTrack*>(d_trk.p), static_cast<float*>(d_histo.p));
+  pv_beamline_peak<<<dim3((N + PV::num_threads_pv_beamline_peak_t - 1) / PV::num_threads_pv_beamline_peak_t),
+                     dim3(PV::num_threads_pv_beamline_peak_t), 0, s>>>(
+    static_cast<float*>(d_histo.p), static_cast<float*>(d_peaks.p), static_cast<uint*>(d_npeaks.p), N);
+  CK(cudaMemsetAsync(d_nvtx.p, 0, 4ull * N, s));
+  pv_beamline_multi_fitter<<<dim3(N), dim3(32), 0, s>>>(
+    static_cast<int*>(d_atomics.p), static_cast<uint*>(d_hn.p), static_cast<PVTrack*>(d_trk.p),
+    static_cast<float*>(d_peaks.p), static_cast<uint*>(d_npeaks.p), static_cast<PV::Vertex*>(d_vtx.p),
+    static_cast<uint*>(d_nvtx.p));
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(s));
+  if (zhisto) CK(cudaMemcpy(zhisto, d_histo.p, 4ull * N * Nbins, cudaMemcpyDeviceToHost));
+  if (zpeaks) CK(cudaMemcpy(zpeaks, d_peaks.p, 4ull * N * PV::max_number_vertices, cudaMemcpyDeviceToHost));
+  if (n_peaks) CK(cudaMemcpy(n_peaks, d_npeaks.p, 4ull * N, cudaMemcpyDeviceToHost));
+  if (vertices)
+    CK(cudaMemcpy(vertices, d_vtx.p, sizeof(PV::Vertex) * N * PV::max_number_vertices, cudaMemcpyDeviceToHost));
+  if (n_vertices) CK(cudaMemcpy(n_vertices, d_nvtx.p, 4ull * N, cudaMemcpyDeviceToHost));
+  cudaStreamDestroy(s);  // the buffers free themselves
+  return 0;
+}
 }
