@@ -243,6 +243,7 @@ def roofline(stages, census, n_events, n_batches, peak, peak_kind, traffic_table
         "search_by_triplet": 16 * clusters + 8 * clusters + 2 * track_hits + 2 * tracks,
         "event_scan": 16 * n_events,
         "consolidate_fit": 34 * track_hits + 98 * tracks + 8 * tracks,
+        "pv_beamline": 49 * tracks,  # the Kalman states read once (the stage is off in both timed forms)
     }
     stage_ms = {k: stages[k] for k in chain.STAGES}
     dominant = max(stage_ms, key=stage_ms.get)
@@ -536,6 +537,48 @@ def reference_gpu(batch):
             "what": "reference cuda/velo kernels compiled for sm_100a, one batch per launch sequence"}
 
 
+def pv_leg(batch, threshold):
+    """The beamline PV stage appended to the plain chain on one batch (device-resident
+    input, graphs, CUDA events per stage), next to the reference's own PV kernels
+    (oracle/_ref) on the same consolidated tracks."""
+    import torch
+    raw = torch.from_numpy(batch.raw).cuda()
+    off = torch.from_numpy(batch.offsets.view(np.int64)).cuda()
+    s = torch.cuda.current_stream().cuda_stream
+    vc = chain.VeloChain(max_events=batch.n_events, max_raw_bytes=int(batch.raw.size) + 4096, use_graphs=True)
+    vc.set_block_threshold(threshold)
+    vc.set_pv(True)
+    vc.set_timing(True)
+    for _ in range(2):
+        vc.run_device(raw.data_ptr(), off.data_ptr(), batch.n_events, s)
+    torch.cuda.synchronize()
+    vc.set_timing(True)
+    for _ in range(5):
+        vc.run_device(raw.data_ptr(), off.data_ptr(), batch.n_events, s)
+    vc.sync()
+    st = vc.stage_times()
+    res = vc.results(clusters=False)
+    vc.close()
+    runs = max(1, st.pop("runs"))
+    pv_ms = st["pv_beamline"] / runs
+    chain_ms = sum(st.values()) / runs
+    n = batch.n_events
+    out = {"events": n, "pv_stage_ms": pv_ms, "pv_events_per_s": n / (pv_ms / 1e3),
+           "chain_with_pv_ms": chain_ms, "chain_with_pv_events_per_s": n / (chain_ms / 1e3),
+           "peaks_per_event": float(res["pv_npeaks"].mean()), "vertices_per_event": float(res["pv_count"].mean()),
+           "timing": "CUDA events around the stage, single stream, mean of 5 runs"}
+    try:
+        import oracle
+        if os.path.exists(oracle.REF_GPU_LIB):
+            r = oracle.ref_pv_run(res["atomics"], res["track_hit_number"], res["kalman_raw"], n, reps=4)
+            out["reference_kernels_ms"] = r["ms"]
+            out["reference_kernels_events_per_s"] = n / (r["ms"] / 1e3)
+            out["reference_vertices_per_event"] = float(r["n_vertices"].mean())
+    except Exception as ex:
+        out["reference_error"] = str(ex)
+    return out
+
+
 # ---------------------------------------------------------------------------
 # reference arm: the CPU implementation on the host cores
 # ---------------------------------------------------------------------------
@@ -615,6 +658,11 @@ def main():
                 result["reference_gpu_b200"] = reference_gpu(b0)
             except Exception as ex:
                 result["reference_gpu_b200"] = {"error": str(ex)}
+            try:
+                result["pv"] = pv_leg(chunks[0].subset(0, min(SIDE_BATCH, chunks[0].n_events)),
+                                      result["config"]["search_mapping"]["block_above_clusters"])
+            except Exception as ex:
+                result["pv"] = {"error": str(ex)}
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

@@ -11,11 +11,13 @@
 //      adds with float atomics into global memory (pv_beamline_histo.cu:14-76), so its bins
 //      carry an arbitrary summation order; these are reproducible. Each bin receives the same
 //      per-track contributions, G(bin) - G(bin - 1) of the polynomial Gaussian integral G;
-//   3. one thread finds the peaks (pv_beamline_peak.cu:3-147) on the shared histogram;
-//   4. warp 0 fits one vertex per seed, a lane per seed (pv_beamline_multi_fitter.cu:6-183),
-//      vertices stored in seed order (the reference appends them with an atomic).
+//   3. warp 0 finds the peaks (pv_beamline_peak.cu:3-147) on the shared histogram: the
+//      proto-clusters from ballots over the bins, their extrema walked a lane each;
+//   4. a warp per seed fits its vertex (pv_beamline_multi_fitter.cu:6-183), the tracks over
+//      the lanes (the reference: a thread per seed), the sums reduced across the warp in a
+//      fixed order; vertices stored in seed order (the reference appends them with an atomic).
 // The float expressions keep the reference's order, so they round as its kernels do under
-// the same compiler flags. Kept as in the reference: a vertex counts every track of its
+// the same compiler flags, except the order of the sums over bins and tracks. Kept as in the reference: a vertex counts every track of its
 // event in n_tracks (the track weights of the fit are not kept), so the 5-track cut applies
 // to the event's track count. Beyond the reference's fixed arrays (32 peaks per event, 32
 // extrema per proto-cluster, 200 cluster edges and clusters, 50 subclusters), where it writes
@@ -97,12 +99,17 @@ struct PvExtremum {
   float value, integral;
 };
 
+constexpr uint32_t kPvMaxToggles = 512;  // changes between empty and filled bins kept
+
 struct PvSmem {
   float histo[kPvWarps][kPvBins];  // per-warp histograms; histo[0] holds the sum
   float zpeaks[kPvMaxVertices];
   uint32_t n_peaks, flags;
-  uint16_t edges[kPvMaxEdges];
+  uint16_t tog[kPvMaxToggles];
+  uint16_t proto[kPvMaxEdges / 2][2];
   uint16_t izmax[kPvMaxClusters];
+  PvVertex vtx[kPvMaxVertices];
+  uint32_t vkeep[kPvMaxVertices];
 };
 
 __global__ void __launch_bounds__(kPvThreads) pv_beamline_kernel(ChainPointers P, PvPointers V)
@@ -174,45 +181,76 @@ __global__ void __launch_bounds__(kPvThreads) pv_beamline_kernel(ChainPointers P
   }
   __syncthreads();
 
-  // ---- 3. peaks (one thread) ----
+  // ---- 3. peaks (warp 0) ----
+  // (a) The reference scans the bins once (pv_beamline_peak.cu:18-41): at every change
+  // between empty and filled bins (starting from "empty" before bin 1) it opens a
+  // proto-cluster, and at the next change it keeps it if the histogram integral since the
+  // opening bin exceeds minTracksInSeed, otherwise drops it. The changes come here from
+  // ballots over the bins; each proto-cluster's integral is summed in bin order by one lane.
+  // (b) Per kept proto-cluster one lane walks its extrema and splits it into subclusters
+  // (:43-119); (c) the cluster means (:128-137), in bin order.
   const float* zh = s.histo[0];
-  if (threadIdx.x == 0) {
+  if (warp == 0) {
     uint32_t flags = 0;
-    uint32_t n_edges = 0, n_clusters = 0;
-    {
-      const float inv_max_err = 1.f / (10.f * kPvMaxTrackZ0Err);
-      const float threshold = kPvDz * inv_max_err;
-      bool prevempty = true;
-      float integral = zh[0];
-      for (uint16_t i = 1; i < kPvBins; ++i) {
-        integral += zh[i];
+    const float inv_max_err = 1.f / (10.f * kPvMaxTrackZ0Err);
+    const float threshold = kPvDz * inv_max_err;
+    uint32_t n_tog = 0;
+    for (uint32_t c = 0; c < (kPvBins + 31) / 32; ++c) {
+      const int i = static_cast<int>(c * 32 + lane);
+      bool tog = false;
+      if (i >= 1 && i < kPvBins) {
         const bool empty = zh[i] < threshold;
-        if (empty != prevempty) {
-          if (prevempty || integral > kPvMinTracksInSeed) {
-            if (n_edges < kPvMaxEdges) s.edges[n_edges] = i;
-            else flags |= kStatusPvOverflow;
-            ++n_edges;
-          } else {
-            --n_edges;
-          }
-          prevempty = empty;
-          integral = 0;
+        const bool prev = i == 1 ? true : zh[i - 1] < threshold;
+        tog = empty != prev;
+      }
+      const uint32_t bal = __ballot_sync(0xFFFFFFFFu, tog);
+      if (tog) {
+        const uint32_t k = n_tog + __popc(bal & ((1u << lane) - 1u));
+        if (k < kPvMaxToggles) s.tog[k] = static_cast<uint16_t>(i);
+      }
+      n_tog += __popc(bal);
+    }
+    __syncwarp();  // the toggles written by other lanes are read below
+    if (n_tog > kPvMaxToggles) flags |= kStatusPvOverflow;
+    const uint32_t n_open = min(n_tog, kPvMaxToggles) / 2;  // toggles alternate: open, close
+    uint32_t n_proto = 0;
+    for (uint32_t m0 = 0; m0 < n_open; m0 += 32) {
+      const uint32_t m = m0 + lane;
+      bool keep = false;
+      if (m < n_open) {
+        float integral = 0;
+        for (uint32_t j = s.tog[2 * m] + 1u; j <= s.tog[2 * m + 1]; ++j) integral += zh[j];
+        keep = integral > kPvMinTracksInSeed;
+      }
+      const uint32_t bal = __ballot_sync(0xFFFFFFFFu, keep);
+      if (keep) {
+        const uint32_t k = n_proto + __popc(bal & ((1u << lane) - 1u));
+        if (k < kPvMaxEdges / 2) {
+          s.proto[k][0] = s.tog[2 * m];
+          s.proto[k][1] = s.tog[2 * m + 1];
         }
       }
+      n_proto += __popc(bal);
     }
-    const uint32_t n_proto = min(n_edges, kPvMaxEdges) / 2;
+    __syncwarp();
+    if (n_proto > kPvMaxEdges / 2) flags |= kStatusPvOverflow;
+    n_proto = min(n_proto, kPvMaxEdges / 2);
     const float mindip = kPvMinDipDensity * kPvDz;
     const float minpeak = kPvMinDensity * kPvDz;
-    for (uint32_t c = 0; c < n_proto; ++c) {
-      const uint16_t ibegin = s.edges[2 * c], iend = s.edges[2 * c + 1];
-      PvExtremum ex[kPvMaxVertices];
-      int n_ex = 0;
-      auto push = [&](uint16_t idx, float value, float integ) {
-        if (n_ex < static_cast<int>(kPvMaxVertices)) ex[n_ex] = PvExtremum{idx, value, integ};
-        else flags |= kStatusPvOverflow;
-        ++n_ex;
-      };
-      {
+    uint32_t n_clusters = 0;
+    for (uint32_t p0 = 0; p0 < n_proto; p0 += 32) {
+      const uint32_t pc = p0 + lane;
+      uint16_t izm[kPvMaxSubclusters];
+      uint32_t nz = 0;
+      if (pc < n_proto) {
+        const uint16_t ibegin = s.proto[pc][0], iend = s.proto[pc][1];
+        PvExtremum ex[kPvMaxVertices];
+        int n_ex = 0;
+        auto push = [&](uint16_t idx, float value, float integ) {
+          if (n_ex < static_cast<int>(kPvMaxVertices)) ex[n_ex] = PvExtremum{idx, value, integ};
+          else flags |= kStatusPvOverflow;
+          ++n_ex;
+        };
         bool rising = true;
         float integral = zh[ibegin];
         push(ibegin, zh[ibegin], integral);
@@ -242,43 +280,48 @@ __global__ void __launch_bounds__(kPvThreads) pv_beamline_kernel(ChainPointers P
           integral += value;
         }
         push(iend, zh[iend], integral);
-      }
-      const int n = min(n_ex, static_cast<int>(kPvMaxVertices));
-      uint32_t n_sub = 0;
-      uint16_t sub_izmax[kPvMaxSubclusters];
-      if (n > 3) {
-        for (int i = 1; i < n / 2 + 1; ++i) {
-          if (2 * i < n && ex[2 * i].integral - ex[2 * i - 2].integral > kPvMinTracksInSeed) {
-            if (n_sub < kPvMaxSubclusters) sub_izmax[n_sub++] = ex[2 * i - 1].index;
-            else flags |= kStatusPvOverflow;
+        const int n = min(n_ex, static_cast<int>(kPvMaxVertices));
+        if (n > 3) {
+          for (int i = 1; i < n / 2 + 1; ++i) {
+            if (2 * i < n && ex[2 * i].integral - ex[2 * i - 2].integral > kPvMinTracksInSeed) {
+              if (nz < kPvMaxSubclusters) izm[nz++] = ex[2 * i - 1].index;
+              else flags |= kStatusPvOverflow;
+            }
           }
         }
+        if (nz == 0 && n > 1 && ex[1].value >= minpeak) izm[nz++] = ex[1].index;
       }
-      if (n_sub == 0) {
-        if (n > 1 && ex[1].value >= minpeak) {
-          if (n_clusters < kPvMaxClusters) s.izmax[n_clusters++] = ex[1].index;
-          else flags |= kStatusPvOverflow;
-        }
-      } else {
-        for (uint32_t i = 0; i < n_sub; ++i) {
-          if (n_clusters < kPvMaxClusters) s.izmax[n_clusters++] = sub_izmax[i];
-          else flags |= kStatusPvOverflow;
-        }
+      // clusters in proto-cluster order
+      uint32_t incl = nz;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= static_cast<uint32_t>(o)) incl += t;
       }
+      for (uint32_t j = 0; j < nz; ++j) {
+        const uint32_t k = n_clusters + incl - nz + j;
+        if (k < kPvMaxClusters) s.izmax[k] = izm[j];
+      }
+      n_clusters += __shfl_sync(0xFFFFFFFFu, incl, 31);
     }
-    // cluster means (zClusterMean, pv_beamline_peak.cu:128-137)
-    uint32_t n_peaks = 0;
-    for (uint32_t c = 0; c < n_clusters; ++c) {
-      const uint16_t izmax = s.izmax[c];
+    __syncwarp();
+    if (n_clusters > kPvMaxClusters) flags |= kStatusPvOverflow;
+    n_clusters = min(n_clusters, kPvMaxClusters);
+    if (n_clusters > kPvMaxVertices) flags |= kStatusPvOverflow;
+    const uint32_t n_peaks = min(n_clusters, kPvMaxVertices);
+    if (lane < n_peaks) {
+      const uint16_t izmax = s.izmax[lane];
       const float* b = zh + izmax;
       const float d1 = *b - *(b - 1);
       const float d2 = *b - *(b + 1);
       const float idz = d1 + d2 > 0 ? 0.5f * (d1 - d2) / (d1 + d2) : 0.0f;
-      if (n_peaks < kPvMaxVertices) s.zpeaks[n_peaks++] = kPvZmin + kPvDz * (izmax + idz + 0.5f);
-      else flags |= kStatusPvOverflow;
+      s.zpeaks[lane] = kPvZmin + kPvDz * (izmax + idz + 0.5f);
     }
-    s.n_peaks = n_peaks;
-    s.flags = flags;
+    flags = __reduce_or_sync(0xFFFFFFFFu, flags);
+    if (lane == 0) {
+      s.n_peaks = n_peaks;
+      s.flags = flags;
+    }
   }
   __syncthreads();
   if (threadIdx.x < kPvMaxVertices)  // slots past the peaks hold 0
@@ -288,107 +331,120 @@ __global__ void __launch_bounds__(kPvThreads) pv_beamline_kernel(ChainPointers P
     if (s.flags) P.status[e] |= s.flags;
   }
 
-  // ---- 4. multi-vertex fit: warp 0, a lane per seed ----
-  if (warp != 0) return;
+  // ---- 4. multi-vertex fit (pv_beamline_multi_fitter.cu:34-181): a warp per seed, the
+  // tracks over the lanes, sums reduced across the warp in a fixed order ----
   const uint32_t n_seeds = s.n_peaks;
-  PvVertex vertex{};  // one per lane for all its seeds, as in the reference
-  uint32_t stored = 0;
-  for (uint32_t seed0 = 0; seed0 < n_seeds; seed0 += 32) {
-    const uint32_t seed = seed0 + lane;
-    bool keep = false;
-    if (seed < n_seeds) {
-      bool converged = false;
-      float vtxcov[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-      float vx = 0.f, vy = 0.f;
-      float vz = s.zpeaks[seed];
-      const float max_dz_converged = 0.001f;
-      float chi2tot = 0.f;
+  for (uint32_t seed = warp; seed < n_seeds; seed += kPvWarps) {
+    bool converged = false;
+    float vtxcov[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    float vx = 0.f, vy = 0.f;
+    float vz = s.zpeaks[seed];
+    const float max_dz_converged = 0.001f;
+    float chi2tot = 0.f;
+    for (uint32_t iter = 0; iter < kPvMaxFitIter && !converged; ++iter) {
+      float a00 = 0.f, a11 = 0.f, a20 = 0.f, a21 = 0.f, a22 = 0.f;
+      float gx = 0.f, gy = 0.f, gz = 0.f, c2 = 0.f;
       uint32_t nselected = 0;
-      for (uint32_t iter = 0; iter < kPvMaxFitIter && !converged; ++iter) {
-        float a00 = 0.f, a11 = 0.f, a20 = 0.f, a21 = 0.f, a22 = 0.f;
-        float gx = 0.f, gy = 0.f, gz = 0.f;
-        chi2tot = 0.f;
-        nselected = 0;
-        for (uint32_t i = 0; i < nt; ++i) {
-          const PvTrack t = tracks[i];
-          if (kPvZmin > t.z || t.z > kPvZmax) continue;
-          const float dz = vz - t.z;
-          const float rx = vx - (t.x + t.tx * dz);
-          const float ry = vy - (t.y + t.ty * dz);
-          const float chi2 = rx * rx * t.w00 + ry * ry * t.w11;
-          if (chi2 < kPvMaxDeltaChi2) {
-            ++nselected;
-            const float chi2_cut = 0.1f + 0.01f * kPvMaxFitIter / (iter + 1);
-            float weight = expf(-chi2 * 0.5f);
-            float denom = expf(-chi2_cut * 0.5f);
-            for (uint32_t o = 0; o < n_seeds; ++o) {
-              const float odz = s.zpeaks[o] - t.z;
-              const float ox = 0.f - (t.x + t.tx * odz);
-              const float oy = 0.f - (t.y + t.ty * odz);
-              const float ochi2 = ox * ox * t.w00 + oy * oy * t.w11;
-              denom += expf(-ochi2 * 0.5f);
-            }
-            weight = weight / denom;
-            if (weight < kPvMinWeight) continue;
-            const float hx = rx * t.w00;
-            const float hy = ry * t.w11;
-            const float hz = -t.tx * rx * t.w00 - t.ty * ry * t.w11;
-            gx = gx + hx * weight;
-            gy = gy + hy * weight;
-            gz = gz + hz * weight;
-            // HWH of PVTrackInVertex (TrackBeamLineVertexFinder.cuh:57-75)
-            const float h20 = -t.tx, h21 = -t.ty;
-            a00 += weight * t.w00;
-            a11 += weight * t.w11;
-            a20 += weight * (h20 * t.w00);
-            a21 += weight * (h21 * t.w11);
-            a22 += weight * (h20 * h20 * t.w00 + h21 * h21 * t.w11);
-            chi2tot += weight * chi2;
+      const float chi2_cut = 0.1f + 0.01f * kPvMaxFitIter / (iter + 1);
+      const float denom0 = expf(-chi2_cut * 0.5f);
+      for (uint32_t i = lane; i < nt; i += 32) {
+        const PvTrack t = tracks[i];
+        if (kPvZmin > t.z || t.z > kPvZmax) continue;
+        const float dz = vz - t.z;
+        const float rx = vx - (t.x + t.tx * dz);
+        const float ry = vy - (t.y + t.ty * dz);
+        const float chi2 = rx * rx * t.w00 + ry * ry * t.w11;
+        if (chi2 < kPvMaxDeltaChi2) {
+          ++nselected;
+          float weight = expf(-chi2 * 0.5f);
+          float denom = denom0;
+          for (uint32_t o = 0; o < n_seeds; ++o) {
+            const float odz = s.zpeaks[o] - t.z;
+            const float ox = 0.f - (t.x + t.tx * odz);
+            const float oy = 0.f - (t.y + t.ty * odz);
+            const float ochi2 = ox * ox * t.w00 + oy * oy * t.w11;
+            denom += expf(-ochi2 * 0.5f);
           }
-        }
-        if (nselected >= 2) {
-          const float det = a00 * (a22 * a11 - a21 * a21) + a20 * (-a11 * a20);
-          const float inv_det = 1.f / det;
-          vtxcov[0] = (a22 * a11 - a21 * a21) * inv_det;
-          vtxcov[1] = -(-a20 * a21) * inv_det;
-          vtxcov[2] = (a22 * a00 - a20 * a20) * inv_det;
-          vtxcov[3] = (-a20 * a11) * inv_det;
-          vtxcov[4] = -(a21 * a00) * inv_det;
-          vtxcov[5] = (a11 * a00) * inv_det;
-          const float dx = -1.f * (vtxcov[0] * gx + vtxcov[1] * gy + vtxcov[3] * gz);
-          const float dy = -1.f * (vtxcov[1] * gx + vtxcov[2] * gy + vtxcov[4] * gz);
-          const float dzv = -1.f * (vtxcov[3] * gx + vtxcov[4] * gy + vtxcov[5] * gz);
-          chi2tot += dx * gx + dy * gy + dzv * gz;
-          vx = vx + dx;
-          vy = vy + dy;
-          vz = vz + dzv;
-          converged = fabsf(dzv) < max_dz_converged;
-        } else {
-          break;  // the reference's placeholder position is overwritten below
+          weight = weight / denom;
+          if (weight < kPvMinWeight) continue;
+          const float hx = rx * t.w00;
+          const float hy = ry * t.w11;
+          const float hz = -t.tx * rx * t.w00 - t.ty * ry * t.w11;
+          gx = gx + hx * weight;
+          gy = gy + hy * weight;
+          gz = gz + hz * weight;
+          // HWH of PVTrackInVertex (TrackBeamLineVertexFinder.cuh:57-75)
+          const float h20 = -t.tx, h21 = -t.ty;
+          a00 += weight * t.w00;
+          a11 += weight * t.w11;
+          a20 += weight * (h20 * t.w00);
+          a21 += weight * (h21 * t.w11);
+          a22 += weight * (h20 * h20 * t.w00 + h21 * h21 * t.w11);
+          c2 += weight * chi2;
         }
       }
-      vertex.chi2 = chi2tot;
-      vertex.x = vx;
-      vertex.y = vy;
-      vertex.z = vz;
-      vertex.cov00 = vtxcov[0];
-      vertex.cov10 = vtxcov[1];
-      vertex.cov11 = vtxcov[2];
-      vertex.cov20 = vtxcov[3];
-      vertex.cov21 = vtxcov[4];
-      vertex.cov22 = vtxcov[5];
-      vertex.n_tracks += nt;  // every track of the event (weights of fresh track copies are 1)
-      const float rho2 = vertex.x * vertex.x + vertex.y * vertex.y;
-      keep = vertex.n_tracks >= kPvMinTracksPerVertex && rho2 < kPvMaxVertexRho2;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        a00 += __shfl_xor_sync(0xFFFFFFFFu, a00, o);
+        a11 += __shfl_xor_sync(0xFFFFFFFFu, a11, o);
+        a20 += __shfl_xor_sync(0xFFFFFFFFu, a20, o);
+        a21 += __shfl_xor_sync(0xFFFFFFFFu, a21, o);
+        a22 += __shfl_xor_sync(0xFFFFFFFFu, a22, o);
+        gx += __shfl_xor_sync(0xFFFFFFFFu, gx, o);
+        gy += __shfl_xor_sync(0xFFFFFFFFu, gy, o);
+        gz += __shfl_xor_sync(0xFFFFFFFFu, gz, o);
+        c2 += __shfl_xor_sync(0xFFFFFFFFu, c2, o);
+        nselected += __shfl_xor_sync(0xFFFFFFFFu, nselected, o);
+      }
+      chi2tot = c2;
+      if (nselected >= 2) {
+        const float det = a00 * (a22 * a11 - a21 * a21) + a20 * (-a11 * a20);
+        const float inv_det = 1.f / det;
+        vtxcov[0] = (a22 * a11 - a21 * a21) * inv_det;
+        vtxcov[1] = -(-a20 * a21) * inv_det;
+        vtxcov[2] = (a22 * a00 - a20 * a20) * inv_det;
+        vtxcov[3] = (-a20 * a11) * inv_det;
+        vtxcov[4] = -(a21 * a00) * inv_det;
+        vtxcov[5] = (a11 * a00) * inv_det;
+        const float dx = -1.f * (vtxcov[0] * gx + vtxcov[1] * gy + vtxcov[3] * gz);
+        const float dy = -1.f * (vtxcov[1] * gx + vtxcov[2] * gy + vtxcov[4] * gz);
+        const float dzv = -1.f * (vtxcov[3] * gx + vtxcov[4] * gy + vtxcov[5] * gz);
+        chi2tot += dx * gx + dy * gy + dzv * gz;
+        vx = vx + dx;
+        vy = vy + dy;
+        vz = vz + dzv;
+        converged = fabsf(dzv) < max_dz_converged;
+      } else {
+        break;  // the reference's placeholder position is overwritten below
+      }
     }
-    uint32_t n_keep;
-    const uint32_t b = __ballot_sync(0xFFFFFFFFu, keep);
-    n_keep = __popc(b);
-    if (keep) V.vertices[e * kPvMaxVertices + stored + __popc(b & ((1u << lane) - 1u))] = vertex;
-    stored += n_keep;
+    if (lane == 0) {
+      PvVertex v{};
+      v.chi2 = chi2tot;
+      v.x = vx;
+      v.y = vy;
+      v.z = vz;
+      v.cov00 = vtxcov[0];
+      v.cov10 = vtxcov[1];
+      v.cov11 = vtxcov[2];
+      v.cov20 = vtxcov[3];
+      v.cov21 = vtxcov[4];
+      v.cov22 = vtxcov[5];
+      v.n_tracks = nt;  // every track of the event (the weights of fresh track copies are 1)
+      s.vtx[seed] = v;
+      s.vkeep[seed] = nt >= kPvMinTracksPerVertex && v.x * v.x + v.y * v.y < kPvMaxVertexRho2;
+    }
   }
-  for (uint32_t k = stored + lane; k < kPvMaxVertices; k += 32) V.vertices[e * kPvMaxVertices + k] = PvVertex{};
-  if (lane == 0) V.n_vertices[e] = stored;
+  __syncthreads();
+  // kept vertices in seed order (the reference appends them with an atomic)
+  if (warp == 0) {
+    const bool keep = lane < n_seeds && s.vkeep[lane];
+    const uint32_t bal = __ballot_sync(0xFFFFFFFFu, keep);
+    const uint32_t stored = __popc(bal);
+    if (keep) V.vertices[e * kPvMaxVertices + __popc(bal & ((1u << lane) - 1u))] = s.vtx[lane];
+    if (lane >= stored) V.vertices[e * kPvMaxVertices + lane] = PvVertex{};
+    if (lane == 0) V.n_vertices[e] = stored;
+  }
 }
 
 }  // namespace velo

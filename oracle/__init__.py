@@ -152,7 +152,7 @@ def ref_gpu_lib():
         L.ref_free.argtypes = [C.POINTER(RefOutputs)]
         L.ref_state_size.restype = C.c_int
         L.ref_pv_vertex_size.restype = C.c_int
-        L.ref_pv_run.argtypes = [P, P, P, C.c_uint32, P, P, P, P, P]
+        L.ref_pv_run.argtypes = [P, P, P, C.c_uint32, P, P, P, P, P, C.c_int, C.POINTER(C.c_float)]
         L.ref_pv_run.restype = C.c_int
         _ref_gpu = L
     return _ref_gpu
@@ -201,11 +201,12 @@ def ref_gpu_run(batch, geometry, reps=1):
 REF_PV_NBINS, REF_PV_MAX_VERTICES = 2400, 32
 
 
-def ref_pv_run(atomics, track_hit_number, kalman_raw, n_events):
+def ref_pv_run(atomics, track_hit_number, kalman_raw, n_events, reps=1):
     """The reference's beamline PV kernels (cuda/PV/beamlinePV) on consolidated VELO tracks:
     atomics[2N+1], track_hit_number[T+1], Kalman states as raw bytes (sizeof(VeloState) * T).
     Returns dict zhisto [N, 2400], zpeaks [N, 32], n_peaks [N], vertices (raw bytes,
-    PV::Vertex [N, 32]), n_vertices [N]."""
+    PV::Vertex [N, 32]), n_vertices [N], ms (device time of the four kernels, mean over
+    reps - 1 repetitions after the first when reps > 1)."""
     L = ref_gpu_lib()
     N = int(n_events)
     a = np.ascontiguousarray(atomics, np.uint32)
@@ -215,12 +216,14 @@ def ref_pv_run(atomics, track_hit_number, kalman_raw, n_events):
     out = dict(zhisto=np.zeros((N, REF_PV_NBINS), np.float32), zpeaks=np.zeros((N, REF_PV_MAX_VERTICES), np.float32),
                n_peaks=np.zeros(N, np.uint32), vertices=np.zeros(N * REF_PV_MAX_VERTICES * vs, np.uint8),
                n_vertices=np.zeros(N, np.uint32))
+    ms = C.c_float()
     rc = L.ref_pv_run(a.ctypes.data, thn.ctypes.data, kal.ctypes.data, N, out["zhisto"].ctypes.data,
                       out["zpeaks"].ctypes.data, out["n_peaks"].ctypes.data, out["vertices"].ctypes.data,
-                      out["n_vertices"].ctypes.data)
+                      out["n_vertices"].ctypes.data, int(reps), C.byref(ms))
     if rc != 0:
         raise RuntimeError(f"ref_pv_run failed: {rc}")
     out["vertex_size"] = vs
+    out["ms"] = ms.value
     return out
 
 

@@ -331,7 +331,8 @@ int ref_pv_vertex_size(void) { return static_cast<int>(sizeof(PV::Vertex)); }
 // and the vertex-count memset of stream/visitors/beamlinePV/src/*.cu. Outputs: the z
 // histograms [N * Nbins], peaks [N * 32] with counts [N], vertices [N * 32] with counts [N].
 int ref_pv_run(const uint32_t* atomics, const uint32_t* track_hit_number, const void* kalman, uint32_t n_events,
-               float* zhisto, float* zpeaks, uint32_t* n_peaks, void* vertices, uint32_t* n_vertices)
+               float* zhisto, float* zpeaks, uint32_t* n_peaks, void* vertices, uint32_t* n_vertices, int reps,
+               float* ms_per_rep)
 {
   if (!atomics || !track_hit_number || !kalman || n_events == 0) return -1;
   const uint32_t N = n_events, T = atomics[2 * N];
@@ -350,6 +351,12 @@ int ref_pv_run(const uint32_t* atomics, const uint32_t* track_hit_number, const 
   CK(cudaMemcpy(d_atomics.p, atomics, 4ull * (2 * N + 1), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(d_hn.p, track_hit_number, 4ull * (T + 1), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(d_kal.p, kalman, sizeof(VeloState) * T, cudaMemcpyHostToDevice));
+  cudaEvent_t t0, t1;
+  CK(cudaEventCreate(&t0));
+  CK(cudaEventCreate(&t1));
+  float total_ms = 0.f;
+  for (int rep = 0; rep < (reps > 0 ? reps : 1); ++rep) {
+  CK(cudaEventRecord(t0, s));
   pv_beamline_extrapolate<<<dim3(N), dim3(128), 0, s>>>(static_cast<char*>(d_kal.p), static_cast<int*>(d_atomics.p),
                                                         static_cast<uint*>(d_hn.p), static_cast<PVTrack*>(d_trk.p));
   pv_beamline_histo<<<dim3(N), dim3(128), 0, s>>>(static_cast<int*>(d_atomics.p), static_cast<uint*>(d_hn.p),
@@ -362,8 +369,16 @@ int ref_pv_run(const uint32_t* atomics, const uint32_t* track_hit_number, const 
     static_cast<int*>(d_atomics.p), static_cast<uint*>(d_hn.p), static_cast<PVTrack*>(d_trk.p),
     static_cast<float*>(d_peaks.p), static_cast<uint*>(d_npeaks.p), static_cast<PV::Vertex*>(d_vtx.p),
     static_cast<uint*>(d_nvtx.p));
+  CK(cudaEventRecord(t1, s));
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(s));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, t0, t1));
+  if (rep > 0 || reps <= 1) total_ms += ms;  // the first of several repetitions warms up
+  }
+  if (ms_per_rep) *ms_per_rep = total_ms / (reps > 1 ? reps - 1 : 1);
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
   if (zhisto) CK(cudaMemcpy(zhisto, d_histo.p, 4ull * N * Nbins, cudaMemcpyDeviceToHost));
   if (zpeaks) CK(cudaMemcpy(zpeaks, d_peaks.p, 4ull * N * PV::max_number_vertices, cudaMemcpyDeviceToHost));
   if (n_peaks) CK(cudaMemcpy(n_peaks, d_npeaks.p, 4ull * N, cudaMemcpyDeviceToHost));
