@@ -289,22 +289,46 @@ __global__ void __launch_bounds__(WPB * 32) consolidate_fit_kernel(ChainPointers
     __syncwarp();
     // coalesced write of the chunk's hit range [carry, carry + chunk_hits)
     const bool staged = chunk_hits <= kConsolidateStage;
-    for (uint32_t j = lane; j < chunk_hits; j += 32) {
-      uint32_t lo = 0, hi = 32;  // last track with s_off <= j
-      while (hi - lo > 1) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (s_off[warp][mid] <= j) lo = mid; else hi = mid;
+    // four output positions per lane at a time: their dependent gathers (hit index, then
+    // record and id) are in flight together
+    for (uint32_t j0 = lane; j0 < chunk_hits; j0 += 4 * 32) {
+      uint32_t hh[4];
+#pragma unroll
+      for (uint32_t u = 0; u < 4; ++u) {
+        const uint32_t j = j0 + 32 * u;
+        hh[u] = 0;
+        if (j < chunk_hits) {
+          uint32_t lo = 0, hi = 32;  // last track with s_off <= j
+          while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (s_off[warp][mid] <= j) lo = mid; else hi = mid;
+          }
+          hh[u] = track_hits[(i0 + lo) * kMaxTrackSize + (j - s_off[warp][lo])];
+        }
       }
-      const uint32_t h = track_hits[(i0 + lo) * kMaxTrackSize + (j - s_off[warp][lo])];
-      const float4 p = H[h];
-      ox[carry + j] = p.x;
-      oy[carry + j] = p.y;
-      oz[carry + j] = p.z;
-      oid[carry + j] = ids[h];
-      if (staged) {
-        s_hit[warp][0][j] = p.x;
-        s_hit[warp][1][j] = p.y;
-        s_hit[warp][2][j] = p.z;
+      float4 p[4];
+      uint32_t id[4];
+#pragma unroll
+      for (uint32_t u = 0; u < 4; ++u) {
+        if (j0 + 32 * u < chunk_hits) {
+          p[u] = H[hh[u]];
+          id[u] = ids[hh[u]];
+        }
+      }
+#pragma unroll
+      for (uint32_t u = 0; u < 4; ++u) {
+        const uint32_t j = j0 + 32 * u;
+        if (j < chunk_hits) {
+          ox[carry + j] = p[u].x;
+          oy[carry + j] = p[u].y;
+          oz[carry + j] = p[u].z;
+          oid[carry + j] = id[u];
+          if (staged) {
+            s_hit[warp][0][j] = p[u].x;
+            s_hit[warp][1][j] = p[u].y;
+            s_hit[warp][2][j] = p[u].z;
+          }
+        }
       }
     }
     __syncwarp();

@@ -5,12 +5,12 @@
 //   1. every track is extrapolated to its point of closest approach to the beamline
 //      (pv_beamline_extrapolate.cu:3-30, the PVTrack constructor of
 //      TrackBeamLineVertexFinder.cuh:9-31) into a scratch array;
-//   2. the z histogram (2400 bins of 0.25 mm) lives in shared memory only: each warp adds
-//      its share of the tracks, in track order, into a histogram of its own (a track's bins
-//      over the lanes), and the four are summed bin by bin in a fixed order. The reference
-//      adds with float atomics into global memory (pv_beamline_histo.cu:14-76), so its bins
-//      carry an arbitrary summation order; these are reproducible. Each bin receives the same
-//      per-track contributions, G(bin) - G(bin - 1) of the polynomial Gaussian integral G;
+//   2. the z histogram (2400 bins of 0.25 mm) lives in shared memory only: each warp owns a
+//      quarter of the bins and adds every track's contributions to them, tracks in order, a
+//      track's bins over the lanes. The reference adds with float atomics into global memory
+//      (pv_beamline_histo.cu:14-76), so its bins carry an arbitrary summation order; these
+//      are reproducible. Each bin receives the same per-track contributions,
+//      G(bin) - G(bin - 1) of the polynomial Gaussian integral G;
 //   3. warp 0 finds the peaks (pv_beamline_peak.cu:3-147) on the shared histogram: the
 //      proto-clusters from ballots over the bins, their extrema walked a lane each;
 //   4. a warp per seed fits its vertex (pv_beamline_multi_fitter.cu:6-183), the tracks over
@@ -101,8 +101,10 @@ struct PvExtremum {
 
 constexpr uint32_t kPvMaxToggles = 512;  // changes between empty and filled bins kept
 
+constexpr int kPvBinsPerWarp = kPvBins / kPvWarps;
+
 struct PvSmem {
-  float histo[kPvWarps][kPvBins];  // per-warp histograms; histo[0] holds the sum
+  float histo[kPvBins];
   float zpeaks[kPvMaxVertices];
   uint32_t n_peaks, flags;
   uint16_t tog[kPvMaxToggles];
@@ -146,17 +148,18 @@ __global__ void __launch_bounds__(kPvThreads) pv_beamline_kernel(ChainPointers P
     t.w11 = 1.f / a11;
     tracks[i] = t;
   }
-  for (uint32_t b = threadIdx.x; b < kPvWarps * kPvBins; b += kPvThreads) (&s.histo[0][0])[b] = 0.f;
+  for (uint32_t b = threadIdx.x; b < kPvBins; b += kPvThreads) s.histo[b] = 0.f;
   if (threadIdx.x == 0) {
     s.n_peaks = 0;
     s.flags = 0;
   }
   __syncthreads();
 
-  // ---- 2. z histogram: warp w adds tracks w, w + 4, ... in order, one bin per lane ----
+  // ---- 2. z histogram: warp w fills bins [w * 600, (w + 1) * 600) from every track, in order ----
   {
-    float* h = s.histo[warp];
-    for (uint32_t i = warp; i < nt; i += kPvWarps) {
+    float* h = s.histo;
+    const int own_lo = static_cast<int>(warp) * kPvBinsPerWarp, own_hi = own_lo + kPvBinsPerWarp - 1;
+    for (uint32_t i = 0; i < nt; ++i) {
       const PvTrack t = tracks[i];
       if (!(kPvZmin < t.z && t.z < kPvZmax)) continue;
       const float zbin = (t.z - kPvZmin) / kPvDz;
@@ -167,17 +170,11 @@ __global__ void __launch_bounds__(kPvThreads) pv_beamline_kernel(ChainPointers P
       const float halfwindow = a * zerr / kPvDz;
       const int minbin = max(int(zbin - halfwindow), 1);
       const int maxbin = min(int(zbin + halfwindow), kPvBins - 2);
-      for (int b = minbin + static_cast<int>(lane); b <= maxbin; b += 32)
+      const int first = max(minbin, own_lo), last = min(maxbin, own_hi);
+      for (int b = first + static_cast<int>(lane); b <= last; b += 32)
         h[b] += pv_bin_contribution(t, zerr, minbin, maxbin, b);
       __syncwarp();
     }
-  }
-  __syncthreads();
-  for (uint32_t b = threadIdx.x; b < kPvBins; b += kPvThreads) {
-    float v = s.histo[0][b];
-#pragma unroll
-    for (uint32_t w = 1; w < kPvWarps; ++w) v += s.histo[w][b];
-    s.histo[0][b] = v;
   }
   __syncthreads();
 
@@ -189,7 +186,7 @@ __global__ void __launch_bounds__(kPvThreads) pv_beamline_kernel(ChainPointers P
   // ballots over the bins; each proto-cluster's integral is summed in bin order by one lane.
   // (b) Per kept proto-cluster one lane walks its extrema and splits it into subclusters
   // (:43-119); (c) the cluster means (:128-137), in bin order.
-  const float* zh = s.histo[0];
+  const float* zh = s.histo;
   if (warp == 0) {
     uint32_t flags = 0;
     const float inv_max_err = 1.f / (10.f * kPvMaxTrackZ0Err);

@@ -1,7 +1,7 @@
 """Small fixed workload for profiler captures: one batch of nu ~ U(2,15) events, run
 `--runs` times through the chain (device-resident input, no graphs).
 
-python -m cuda_hlt_b200.profile_case [--events 8192] [--runs 2] [--block-threshold N] [--mode plain|pruned]
+python -m cuda_hlt_b200.profile_case [--events 8192] [--runs 2] [--block-threshold N] [--mode plain|pruned] [--pv]
 
 --block-threshold: events with more clusters than N use the block-per-event search, the
 others the warp-per-event one (1536 is the context default; 16384 sends every event to
@@ -19,6 +19,7 @@ def main():
     ap.add_argument("--config", default="batched_500k")
     ap.add_argument("--block-threshold", type=int, default=1536)
     ap.add_argument("--mode", default="plain", choices=["plain", "pruned"])
+    ap.add_argument("--pv", action="store_true", help="append the beamline PV stage")
     args = ap.parse_args()
     import torch
     from cuda_hlt_b200 import chain, events
@@ -28,6 +29,7 @@ def main():
     vc = chain.VeloChain(max_events=args.events, max_raw_bytes=int(b.raw.size) + 4096, max_tracks=160 * args.events,
                          max_track_hits=12 * 160 * args.events)
     vc.set_block_threshold(args.block_threshold)
+    vc.set_pv(args.pv)
     if args.mode == "pruned":
         from cuda_hlt_b200 import mlp, train_scorer
         vc.set_mlp(mlp.load_weights(train_scorer.DEFAULT_WEIGHTS))
