@@ -36,7 +36,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-from cuda_hlt_b200 import chain, events  # noqa: E402
+from cuda_hlt_b200 import chain, events, shard  # noqa: E402
 
 METRIC = "VELO events/s on 1 B200, MLP-pruned vs plain at ≤0.2% eff loss; % HBM peak"
 UNIT = "events/s"
@@ -224,9 +224,7 @@ def time_form(vcs, streams, batch_ptrs, args, world, dist, torch, local_rank):
         dist.barrier()
     elapsed_ms = start.elapsed_time(end)
     if world > 1:
-        t = torch.tensor([elapsed_ms], device=torch.device("cuda", local_rank))
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
+        elapsed_ms = shard.max_over_ranks(elapsed_ms, dist, torch.device("cuda", local_rank))
     stages = {}
     for vc in vcs:
         for k, v in vc.stage_times().items():
@@ -299,7 +297,8 @@ def run_ours(args, rank, world, local_rank):
     weights, scorer_info = load_scorer(args)
     t0 = time.time()
     n_events = args.events
-    chunks = generate_workload(rank * n_events, n_events, threads)
+    first_event, n_events = shard.event_range(rank, n_events)
+    chunks = generate_workload(first_event, n_events, threads)
     log(f"[rank {rank}] generated {n_events} events in {time.time() - t0:.1f}s, "
         f"{sum(c.raw.size for c in chunks) / 1e9:.2f} GB raw")
     plan = batch_plan(chunks)
@@ -478,9 +477,7 @@ def run_e2e(args, chunks, plan, local_rank, torch, world, dist, threshold, weigh
     torch.cuda.synchronize()
     el = time.perf_counter() - t0
     if world > 1:
-        t = torch.tensor([el], device=torch.device("cuda", local_rank), dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        el = float(t.item())
+        el = shard.max_over_ranks(el, dist, torch.device("cuda", local_rank))
     for vc in ctxs:
         vc.close()
     for c in chunks:
