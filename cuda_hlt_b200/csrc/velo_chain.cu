@@ -56,6 +56,7 @@ struct VeloCtx {
   uint8_t* d_keep = nullptr;
   uint8_t* d_cand_feat = nullptr;
   uint32_t* d_cand_slot = nullptr;
+  uint2* d_cand_rec = nullptr;
   uint64_t hit_capacity = 0;
   uint32_t *d_module_start = nullptr, *d_module_num = nullptr, *d_event_hit_base = nullptr, *d_event_hits = nullptr,
            *d_status = nullptr;
@@ -88,7 +89,7 @@ struct VeloCtx {
   int decode_warps = 8;
   int search_wpb = 4;
   uint32_t decode_blocks = 0, search_blocks = 0, search_block_blocks = 0, fill_blocks = 0, fill_pruned_blocks = 0,
-           score_blocks = 0;
+           feature_blocks = 0, score_blocks = 0;
   // CUDA graphs per (n_events, raw, offsets)
   struct GraphKey {
     uint32_t n;
@@ -133,7 +134,7 @@ cudaError_t dalloc(T*& p, size_t count)
 void free_all(VeloCtx* c)
 {
   void* ptrs[] = {c->d_geometry, c->d_sp_patterns, c->d_sp_fx, c->d_sp_fy, c->d_sp_sizes, c->d_mlp_w, c->d_mlp_norm,
-                  c->d_hit_size, c->d_windows, c->d_keep, c->d_cand_feat, c->d_cand_slot, c->d_raw, c->d_raw_offsets, c->d_hxyzp,
+                  c->d_hit_size, c->d_windows, c->d_keep, c->d_cand_feat, c->d_cand_slot, c->d_cand_rec, c->d_raw, c->d_raw_offsets, c->d_hxyzp,
                   c->d_hid, c->d_stage_xyzp, c->d_stage_id, c->d_module_start, c->d_module_num, c->d_event_hit_base,
                   c->d_event_hits, c->d_status, c->d_track_n, c->d_track_hits, c->d_tracklets, c->d_weak, c->d_ttf,
                   c->d_event_tracks, c->d_event_track_hits, c->d_atomics, c->d_track_hit_number,
@@ -182,6 +183,7 @@ ChainPointers pointers(VeloCtx* c, const void* raw, const uint64_t* offsets, uin
   P.keep = c->mode == VELO_MODE_PRUNED ? c->d_keep : nullptr;
   P.cand_feat = c->d_cand_feat;
   P.cand_slot = c->d_cand_slot;
+  P.cand_rec = c->d_cand_rec;
   P.scratch = SearchScratch{c->d_track_n, c->d_track_hits, c->d_tracklets, c->d_ttf, c->d_weak};
   P.event_tracks = c->d_event_tracks;
   P.event_track_hits = c->d_event_track_hits;
@@ -229,8 +231,10 @@ int launch_chain(VeloCtx* c, const ChainPointers& P, cudaStream_t s, bool captur
   if (P.keep) {
     fill_candidates_kernel<true><<<std::min<uint32_t>(n, c->fill_pruned_blocks), kFillThreads, 0, s>>>(P);
     VCK(cudaGetLastError());
+    candidate_features_kernel<<<c->feature_blocks, kFillThreads, 0, s>>>(P);
+    VCK(cudaGetLastError());
     score_candidates_kernel<<<c->score_blocks, kMlpTile, kScoreSmem, s>>>(P);
-    c->launches += 2;
+    c->launches += 3;
   } else {
     fill_candidates_kernel<false><<<std::min<uint32_t>(n, c->fill_blocks), kFillThreads, 0, s>>>(P);
     ++c->launches;
@@ -328,6 +332,7 @@ int velo_create(const VeloConfig* cfg, const void* geometry, size_t geometry_byt
   ok &= dalloc(c->d_keep, c->hit_capacity) == cudaSuccess;
   ok &= dalloc(c->d_cand_feat, (c->hit_capacity + kMlpTile) * kMlpK1 * 2) == cudaSuccess;
   ok &= dalloc(c->d_cand_slot, c->hit_capacity) == cudaSuccess;
+  ok &= dalloc(c->d_cand_rec, c->hit_capacity) == cudaSuccess;
   ok &= dalloc(c->d_module_start, static_cast<size_t>(N) * kModules) == cudaSuccess;
   ok &= dalloc(c->d_module_num, static_cast<size_t>(N) * kModules) == cudaSuccess;
   ok &= dalloc(c->d_event_hit_base, N) == cudaSuccess;
@@ -382,6 +387,8 @@ int velo_create(const VeloConfig* cfg, const void* geometry, size_t geometry_byt
   c->fill_blocks = static_cast<uint32_t>(std::max(1, occ) * c->sm_count);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fill_candidates_kernel<true>, kFillThreads, 0);
   c->fill_pruned_blocks = static_cast<uint32_t>(std::max(1, occ) * c->sm_count);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, candidate_features_kernel, kFillThreads, 0);
+  c->feature_blocks = static_cast<uint32_t>(std::max(1, occ) * c->sm_count);
   // the scorer: as many CTAs per SM as shared memory holds (1 KB of it is reserved per
   // block), at most 8 (each holds 64 of the SM's 512 tensor-memory columns)
   cudaFuncSetAttribute(score_candidates_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -5,12 +5,14 @@
 // 3) writes them as event-relative u16 pairs {first, last} (0xFFFF = none), so the search
 // kernel reads a window instead of binary-searching inside its serial module loop.
 //
-// Pruned mode, two kernels:
-//   fill_candidates<true>  also computes the twelve proxy-triplet features of every seeding
-//                          candidate (both windows non-empty) and appends them, normalised
-//                          and in bf16, to a compact list of 128-row tiles laid out for the
-//                          tensor core (queue slot 7 counts the rows), with the candidate's
-//                          hit slot alongside;
+// Pruned mode, three kernels:
+//   fill_candidates<true>  also appends every seeding candidate (both windows non-empty)
+//                          that the scoring gate admits to a compact list, as an 8-byte
+//                          record (event hit base, h1, module; queue slot 7 counts them);
+//   candidate_features     a thread per listed candidate (all lanes busy, full occupancy)
+//                          computes its twelve proxy-triplet features and writes them,
+//                          normalised and in bf16, as a row of 128-row tiles laid out for
+//                          the tensor core, with the candidate's hit slot alongside;
 //   score_candidates       a persistent tcgen05 kernel: each CTA bulk-copies 4 KB tiles of
 //                          that list into shared memory (double-buffered), runs the MLP and
 //                          writes the verdict per candidate: a pruned seed gets its h0 window
@@ -39,9 +41,7 @@ __global__ void __launch_bounds__(kFillThreads) fill_candidates_kernel(ChainPoin
 {
   __shared__ uint32_t s_ms[kModules + 1];
   __shared__ uint32_t s_event;
-  __shared__ float s_norm[32];
   const uint32_t lane = threadIdx.x & 31u;
-  if (kPruned && threadIdx.x < 32) s_norm[threadIdx.x] = P.mlp.norm[threadIdx.x];
 
   for (;;) {
     if (threadIdx.x == 0) s_event = atomicAdd(P.queue + 3, 1u);
@@ -90,19 +90,13 @@ __global__ void __launch_bounds__(kFillThreads) fill_candidates_kernel(ChainPoin
           if (valid) P.keep[base + h] = cand ? 3u : 2u;  // candidates: verdict from score_candidates
           // seeds whose pair loop is cheaper than their scoring stay kept, unscored
           const bool append = cand && !fallback && static_cast<uint32_t>((l0 - f0) * (l2 - f2)) >= P.mlp.min_pairs;
-          // one atomic per warp for the rows of its candidates
+          // one atomic per warp for the rows of its candidates; the features follow in
+          // candidate_features, densely
           const uint32_t bal = __ballot_sync(0xFFFFFFFFu, append);
           uint32_t row0 = 0;
           if (lane == 0 && bal) row0 = atomicAdd(P.queue + 7, static_cast<uint32_t>(__popc(bal)));
           row0 = __shfl_sync(0xFFFFFFFFu, row0, 0);
-          if (append) {
-            const uint32_t r = row0 + __popc(bal & ((1u << lane) - 1u));
-            float f[kMlpFeatures];
-            seed_features(H, P.hit_size + base, h, m, f0, l0, f2, l2, f);
-            store_feature_row(P.cand_feat + static_cast<size_t>(r / kMlpTile) * kCandTileBytes, r % kMlpTile, f,
-                              s_norm);
-            P.cand_slot[r] = base + h;
-          }
+          if (append) P.cand_rec[row0 + __popc(bal & ((1u << lane) - 1u))] = make_uint2(base, h | (m << 16));
         }
       }
     }
@@ -110,6 +104,25 @@ __global__ void __launch_bounds__(kFillThreads) fill_candidates_kernel(ChainPoin
   }
 }
 
+
+// Features of the listed candidates: a thread per row, grid-stride over queue slot 7's rows.
+__global__ void __launch_bounds__(kFillThreads) candidate_features_kernel(ChainPointers P)
+{
+  __shared__ float s_norm[32];
+  if (threadIdx.x < 32) s_norm[threadIdx.x] = P.mlp.norm[threadIdx.x];
+  __syncthreads();
+  const uint32_t rows = P.queue[7];
+  for (uint32_t r = blockIdx.x * kFillThreads + threadIdx.x; r < rows; r += gridDim.x * kFillThreads) {
+    const uint2 c = P.cand_rec[r];
+    const uint32_t base = c.x, h = c.y & 0xFFFFu, m = c.y >> 16;
+    const uint2 w = P.windows[base + h];
+    float f[kMlpFeatures];
+    seed_features(P.hits.xyzp + base, P.hit_size + base, h, m, static_cast<int>(w.x & 0xFFFFu),
+                  static_cast<int>(w.x >> 16), static_cast<int>(w.y & 0xFFFFu), static_cast<int>(w.y >> 16), f);
+    store_feature_row(P.cand_feat + static_cast<size_t>(r / kMlpTile) * kCandTileBytes, r % kMlpTile, f, s_norm);
+    P.cand_slot[r] = base + h;
+  }
+}
 
 // Shared memory of score_candidates: the inference tile buffers (whose X tile is slot 0 of
 // the copy ring) plus kScoreRing - 1 more X tiles, each slot with its barrier. Tiles are

@@ -93,6 +93,7 @@ struct ChainPointers {
   uint8_t* cand_feat;      // pruned mode: bf16 feature rows of the seeding candidates, 128-row
                            // tiles of 4 KB in the tensor core's K-major layout
   uint32_t* cand_slot;     // pruned mode: hit slot of each candidate row
+  uint2* cand_rec;         // pruned mode: {event hit base, h1 | module << 16} of each row
   // search
   SearchScratch scratch;
   uint32_t* event_tracks;      // [N] tracks per event
