@@ -29,7 +29,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_WEIGHTS = os.path.join(HERE, "data", "velo_mlp_weights.bin")
 BATCH = 16384
 THRESHOLDS = (0.1, 0.3, 0.5, 0.7, 0.85)
-MIN_PAIRS = (0, 8, 16, 24)
+MIN_PAIRS = (0, 8, 16, 24, 32)
 
 
 def log(*a):
@@ -74,7 +74,8 @@ def evaluate(weights, batch, timing_reps=3):
     """Plain vs pruned on one MC-carrying batch."""
     out = {}
     for name, mode in (("plain", chain.MODE_PLAIN), ("pruned", chain.MODE_PRUNED)):
-        vc = chain.VeloChain(max_events=batch.n_events, max_raw_bytes=int(batch.raw.size) + 4096)
+        vc = chain.VeloChain(max_events=batch.n_events, max_raw_bytes=int(batch.raw.size) + 4096,
+                             mapping=chain.MAP_WARP)  # the mapping the bench's autotuner keeps
         vc.set_mlp(weights)
         vc.set_mode(mode)
         vc.run_host(batch)  # warm-up
