@@ -46,6 +46,7 @@ STATUS = {
     "bad_raw": 1 << 0, "module_overflow": 1 << 1, "hit_overflow": 1 << 2, "candidate_overflow": 1 << 3,
     "track_overflow": 1 << 4, "ttf_overflow": 1 << 5, "weak_overflow": 1 << 6, "h1_overflow": 1 << 7,
     "big_sp_index": 1 << 8, "mlp_fallback": 1 << 9, "empty_module_read": 1 << 10, "seed_tie": 1 << 11,
+    "block_stage_timeout": 1 << 12, "pv_overflow": 1 << 13,
 }
 # Flags of events whose reference result depends on unchecked buffer spills, reads outside
 # a module or the order of atomics (exact float ties).

@@ -129,3 +129,27 @@ def test_pv_reproducible_and_timed():
     assert on["pv_beamline"] > 0 and off["pv_beamline"] < 0.05 * on["pv_beamline"]
     # PV off leaves the outputs unset; the VELO outputs are unchanged by it
     assert res["pv_count"].sum() > 0
+
+
+def test_pv_on_empty_and_corrupt_events():
+    from test_gpu_chain import _empty_event
+    good = events.generate_config("plain_1k", n_events=3)
+    corrupt = good.event(1).copy().view(np.uint32)
+    corrupt[3] = 0xFFFFFF00  # bank offset far outside the event
+    parts = [good.event(0), _empty_event(), corrupt.view(np.uint8), good.event(2)]
+    b = events.EventBatch(np.concatenate(parts), np.concatenate([[0], np.cumsum([p.size for p in parts])]).astype(np.uint64))
+    res = run_pv(b)
+    assert res["pv_count"][1] == res["pv_count"][2] == 0 and res["pv_npeaks"][1] == res["pv_npeaks"][2] == 0
+    assert res["pv_count"][0] > 0 and res["pv_count"][3] > 0
+    assert not np.any(res["status"] & chain.STATUS["pv_overflow"])
+    clean = run_pv(good)
+    for mine_e, clean_e in ((0, 0), (3, 2)):
+        assert res["pv_count"][mine_e] == clean["pv_count"][clean_e]
+        k = int(res["pv_count"][mine_e])
+        assert res["pv_vertices"][mine_e][:k].tobytes() == clean["pv_vertices"][clean_e][:k].tobytes()
+    # an empty batch with the stage on
+    vc = chain.VeloChain(max_events=4, max_raw_bytes=1 << 16)
+    vc.set_pv(True)
+    vc.run_host(events.EventBatch(np.zeros(0, np.uint8), np.zeros(1, np.uint64)))
+    assert vc.sync() == (0, 0, 0)
+    vc.close()
