@@ -277,6 +277,7 @@ __global__ void __launch_bounds__(WPB * 32) consolidate_fit_kernel(ChainPointers
   for (uint32_t i0 = 0; i0 < nt; i0 += 32) {
     const uint32_t i = i0 + lane;
     const uint32_t n = i < nt ? track_n[i] : 0;
+    const uint32_t n_chunk = min(32u, nt - i0);  // tracks of this chunk
     uint32_t incl = n;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -290,21 +291,23 @@ __global__ void __launch_bounds__(WPB * 32) consolidate_fit_kernel(ChainPointers
     // coalesced write of the chunk's hit range [carry, carry + chunk_hits)
     const bool staged = chunk_hits <= kConsolidateStage;
     // four output positions per lane at a time: their dependent gathers (hit index, then
-    // record and id) are in flight together
-    for (uint32_t j0 = lane; j0 < chunk_hits; j0 += 4 * 32) {
+    // record and id) are in flight together. The track of a position: every track has hits,
+    // so the tracks starting inside 32 consecutive positions are marked by one bit each (an
+    // OR across the warp of the lanes' own starts) and counted with a popcount.
+    const uint32_t my_start = lane < n_chunk ? s_off[warp][lane] : 0xFFFFFFFFu;
+    uint32_t started = 0;  // tracks starting before the current group of 32 positions
+    for (uint32_t base = 0; base < chunk_hits; base += 4 * 32) {  // warp-uniform
+      const uint32_t j0 = base + lane;
       uint32_t hh[4];
 #pragma unroll
       for (uint32_t u = 0; u < 4; ++u) {
-        const uint32_t j = j0 + 32 * u;
-        hh[u] = 0;
-        if (j < chunk_hits) {
-          uint32_t lo = 0, hi = 32;  // last track with s_off <= j
-          while (hi - lo > 1) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (s_off[warp][mid] <= j) lo = mid; else hi = mid;
-          }
-          hh[u] = track_hits[(i0 + lo) * kMaxTrackSize + (j - s_off[warp][lo])];
-        }
+        const uint32_t p0 = base + 32 * u;  // first position of this group
+        const uint32_t heads =
+          __reduce_or_sync(0xFFFFFFFFu, my_start - p0 < 32u ? 1u << (my_start - p0) : 0u);
+        const uint32_t j = p0 + lane;
+        const uint32_t t = started + __popc(heads & (0xFFFFFFFFu >> (31 - lane))) - 1;  // track of j
+        started += __popc(heads);
+        hh[u] = j < chunk_hits ? track_hits[(i0 + t) * kMaxTrackSize + (j - s_off[warp][t])] : 0u;
       }
       float4 p[4];
       uint32_t id[4];
