@@ -14,7 +14,7 @@
 //                          normalised and in bf16, as a row of 128-row tiles laid out for
 //                          the tensor core, with the candidate's hit slot alongside;
 //   score_candidates       a persistent tcgen05 kernel: each CTA bulk-copies 4 KB tiles of
-//                          that list into shared memory (double-buffered), runs the MLP and
+//                          those rows into a four-slot shared-memory ring, runs the MLP and
 //                          writes the verdict per candidate: a pruned seed gets its h0 window
 //                          cleared, so the search never sees it; keep bits per hit (bit 0
 //                          seed keep, bit 1 extension keep) are kept for the outputs.
