@@ -246,127 +246,152 @@ __global__ void __launch_bounds__(WPB * 32, 8) search_kernel(ChainPointers P)
       auto seeding = [&](uint32_t first) {
         uint32_t n_h1 = 0;
         const uint32_t tracklets_before = tracklet_ptr;
-        for (int side = 2; side <= 3; ++side) {
-          const uint32_t m = first - side;
-          const uint32_t start = mstart[m], num = mnum[m];
-          for (uint32_t r0 = 0; r0 < num; r0 += kSeedChunk) {
-            const uint32_t r_end = min(num, r0 + kSeedChunk);
-            // (a) unused h1 with both phi windows (FillCandidates.cu:31-68, TrackSeeding.cu:24-49);
-            // the windows of the chunk's (up to) four 32-hit groups are loaded together so that
-            // their latencies overlap
-            uint32_t nc = 0;
-            uint2 wv[kSeedChunk / 32];
+        // Candidates of both modules (first - 2, then first - 3) are queued in the slots and
+        // processed kSeedChunk at a time: a module's last few hits share a pass with the next
+        // module's first ones. The two modules' seeds are independent (seeding marks no hit
+        // used), and winners are appended in queue order, the order of a pass per module.
+        uint32_t nc = 0;  // candidates queued
+        // (b)-(d) on the queued candidates
+        auto flush = [&]() {
+          __syncwarp();
+          // (b) exclusive scan of the h0 counts
+          uint32_t total_pairs = 0;
+          for (uint32_t k0 = 0; k0 < nc; k0 += 32) {
+            const uint32_t k = k0 + lane;
+            const uint32_t v = k < nc ? sl.np[k] : 0;
+            uint32_t incl = v;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+              const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+              if (lane >= static_cast<uint32_t>(o)) incl += t;
+            }
+            if (k < nc) sl.pair_start[k] = total_pairs + incl - v;
+            total_pairs += __shfl_sync(0xFFFFFFFFu, incl, 31);
+          }
+          __syncwarp();
+          // (c) (h1, h0) pairs over the lanes, each scanning its h2 window. Every candidate
+          // has at least one pair (a non-empty window ends past its first hit), so the
+          // candidates starting inside a group of 32 pairs are k_lo + 1 .. k_lo + 32 and
+          // each lane's candidate is k_lo plus the starts at or before it (one shared
+          // load, an OR across the warp and a popcount instead of a binary search).
+          uint32_t k_lo = 0;  // candidate of pair p0
+          for (uint32_t p0 = 0; p0 < total_pairs; p0 += 32) {
+            const uint32_t p = p0 + lane;
+            uint32_t head = 0;
+            if (k_lo + 1 + lane < nc) {
+              const uint32_t s = sl.pair_start[k_lo + 1 + lane];
+              if (s >= p0 && s <= p0 + 31) head = 1u << (s - p0);
+            }
+            const uint32_t heads = __reduce_or_sync(0xFFFFFFFFu, head);
+            const uint32_t k = k_lo + __popc(heads & (0xFFFFFFFFu >> (31 - lane)));
+            k_lo = __shfl_sync(0xFFFFFFFFu, k, 31);
+            if (p < total_pairs) {
+              const uint32_t h0rel = p - sl.pair_start[k];
+              const uint32_t h0i = sl.f0[k] + h0rel;
+              if (!test_used(used, h0i)) {
+                const float4 h0 = H[h0i];
+                const float4 h1 = H[sl.h1[k]];
+                const uint32_t f2 = sl.f2[k], l2 = sl.l2[k];
+                unsigned long long best = ~0ull, last = 0ull;
+                for (uint32_t h2i = f2; h2i < l2; ++h2i) {
+                  if (test_used(used, h2i)) continue;
+                  float scatter;
+                  if (seed_scatter(h0, h1, H[h2i], scatter)) {
+                    const uint32_t idx = (h0rel << 16) | (h2i - f2);
+                    const uint32_t sb = __float_as_uint(scatter);
+                    const unsigned long long key = (static_cast<unsigned long long>(sb) << 32) | idx;
+                    const unsigned long long key_last = (static_cast<unsigned long long>(~sb) << 32) | idx;
+                    best = min(best, key);
+                    last = max(last, key_last);
+                  }
+                }
+                if (best != ~0ull) {
+                  atomicMin(&sl.best[k], best);
+                  atomicMax(&sl.last[k], last);
+                }
+              }
+            }
+          }
+          __syncwarp();
+          // (d) winners, appended in candidate order (TrackSeeding.cu:185-195)
+          for (uint32_t k0 = 0; k0 < nc; k0 += 32) {
+            const uint32_t k = k0 + lane;
+            const bool win = k < nc && sl.best[k] != ~0ull;
+            uint32_t nwin;
+            const uint32_t rank = ballot_rank(win, nwin);
+            if (win) {
+              const unsigned long long key = sl.best[k];
+              if ((key & 0xFFFFFFFFull) != (sl.last[k] & 0xFFFFFFFFull)) flags |= kStatusSeedTie;
+              const uint32_t tp = (tracklet_ptr + rank) % kTrackletRing;
+              tracklets[3 * tp] = static_cast<uint16_t>(sl.f0[k] + ((key >> 16) & 0xFFFFu));
+              tracklets[3 * tp + 1] = sl.h1[k];
+              tracklets[3 * tp + 2] = static_cast<uint16_t>(sl.f2[k] + (key & 0xFFFFu));
+              ttf[(ttf_ptr + rank) % kTtfModulo] = 0x80000000u | tp;
+            }
+            tracklet_ptr += nwin;
+            ttf_ptr += nwin;
+          }
+          __syncwarp();
+          nc = 0;
+        };
+        int side = 2;
+        uint32_t r0 = 0;
+        for (;;) {
+          while (side <= 3 && r0 >= mnum[first - side]) {
+            ++side;
+            r0 = 0;
+          }
+          const bool have = side <= 3;
+          // (a) unused h1 with both phi windows (FillCandidates.cu:31-68, TrackSeeding.cu:24-49)
+          // among the next (up to) kSeedChunk hits; the windows of their 32-hit groups are
+          // loaded together so that their latencies overlap
+          uint32_t start = 0, r_end = 0, n_new = 0;
+          uint2 wv[kSeedChunk / 32];
+          bool hv[kSeedChunk / 32];
+#pragma unroll
+          for (uint32_t j = 0; j < kSeedChunk / 32; ++j) {
+            wv[j] = make_uint2(0xFFFFu, 0xFFFFu);
+            hv[j] = false;
+          }
+          if (have) {
+            const uint32_t m = first - side;
+            start = mstart[m];
+            r_end = min(mnum[m], r0 + kSeedChunk);
 #pragma unroll
             for (uint32_t j = 0; j < kSeedChunk / 32; ++j) {
               const uint32_t r = r0 + 32 * j + lane;
-              wv[j] = make_uint2(0xFFFFu, 0xFFFFu);
               if (r < r_end && !test_used(used, start + r)) wv[j] = Wn[start + r];
             }
 #pragma unroll
             for (uint32_t j = 0; j < kSeedChunk / 32; ++j) {
               const uint32_t r = r0 + 32 * j + lane;
-              const uint32_t h1 = start + r;
-              const uint2 w = wv[j];
-              const int f0 = static_cast<int>(w.x & 0xFFFFu);
-              const int l0 = static_cast<int>(w.x >> 16);
-              const int f2 = static_cast<int>(w.y & 0xFFFFu);
-              const int l2 = static_cast<int>(w.y >> 16);
-              const bool has = r < r_end && f0 != 0xFFFF && f2 != 0xFFFF;
-              uint32_t cnt;
-              const uint32_t rank = ballot_rank(has, cnt);
-              if (has) {
-                const uint32_t k = nc + rank;
-                sl.h1[k] = static_cast<uint16_t>(h1);
-                sl.f0[k] = static_cast<uint16_t>(f0);
-                sl.np[k] = static_cast<uint16_t>(l0 - f0);
-                sl.f2[k] = static_cast<uint16_t>(f2);
-                sl.l2[k] = static_cast<uint16_t>(l2);
-                sl.best[k] = ~0ull;
-                sl.last[k] = 0ull;
-              }
-              nc += cnt;
+              hv[j] = r < r_end && (wv[j].x & 0xFFFFu) != 0xFFFFu && (wv[j].y & 0xFFFFu) != 0xFFFFu;
+              n_new += __popc(__ballot_sync(0xFFFFFFFFu, hv[j]));
             }
-            n_h1 += nc;
-            __syncwarp();
-            // (b) exclusive scan of the h0 counts
-            uint32_t total_pairs = 0;
-            for (uint32_t k0 = 0; k0 < nc; k0 += 32) {
-              const uint32_t k = k0 + lane;
-              const uint32_t v = k < nc ? sl.np[k] : 0;
-              uint32_t incl = v;
-#pragma unroll
-              for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-                if (lane >= static_cast<uint32_t>(o)) incl += t;
-              }
-              if (k < nc) sl.pair_start[k] = total_pairs + incl - v;
-              total_pairs += __shfl_sync(0xFFFFFFFFu, incl, 31);
-            }
-            __syncwarp();
-            // (c) (h1, h0) pairs over the lanes, each scanning its h2 window. Every candidate
-            // has at least one pair (a non-empty window ends past its first hit), so the
-            // candidates starting inside a group of 32 pairs are k_lo + 1 .. k_lo + 32 and
-            // each lane's candidate is k_lo plus the starts at or before it (one shared
-            // load, an OR across the warp and a popcount instead of a binary search).
-            uint32_t k_lo = 0;  // candidate of pair p0
-            for (uint32_t p0 = 0; p0 < total_pairs; p0 += 32) {
-              const uint32_t p = p0 + lane;
-              uint32_t head = 0;
-              if (k_lo + 1 + lane < nc) {
-                const uint32_t s = sl.pair_start[k_lo + 1 + lane];
-                if (s >= p0 && s <= p0 + 31) head = 1u << (s - p0);
-              }
-              const uint32_t heads = __reduce_or_sync(0xFFFFFFFFu, head);
-              const uint32_t k = k_lo + __popc(heads & (0xFFFFFFFFu >> (31 - lane)));
-              k_lo = __shfl_sync(0xFFFFFFFFu, k, 31);
-              if (p < total_pairs) {
-                const uint32_t h0rel = p - sl.pair_start[k];
-                const uint32_t h0i = sl.f0[k] + h0rel;
-                if (!test_used(used, h0i)) {
-                  const float4 h0 = H[h0i];
-                  const float4 h1 = H[sl.h1[k]];
-                  const uint32_t f2 = sl.f2[k], l2 = sl.l2[k];
-                  unsigned long long best = ~0ull, last = 0ull;
-                  for (uint32_t h2i = f2; h2i < l2; ++h2i) {
-                    if (test_used(used, h2i)) continue;
-                    float scatter;
-                    if (seed_scatter(h0, h1, H[h2i], scatter)) {
-                      const uint32_t idx = (h0rel << 16) | (h2i - f2);
-                      const uint32_t sb = __float_as_uint(scatter);
-                      const unsigned long long key = (static_cast<unsigned long long>(sb) << 32) | idx;
-                      const unsigned long long key_last = (static_cast<unsigned long long>(~sb) << 32) | idx;
-                      best = min(best, key);
-                      last = max(last, key_last);
-                    }
-                  }
-                  if (best != ~0ull) {
-                    atomicMin(&sl.best[k], best);
-                    atomicMax(&sl.last[k], last);
-                  }
-                }
-              }
-            }
-            __syncwarp();
-            // (d) winners, appended in candidate order (TrackSeeding.cu:185-195)
-            for (uint32_t k0 = 0; k0 < nc; k0 += 32) {
-              const uint32_t k = k0 + lane;
-              const bool win = k < nc && sl.best[k] != ~0ull;
-              uint32_t nwin;
-              const uint32_t rank = ballot_rank(win, nwin);
-              if (win) {
-                const unsigned long long key = sl.best[k];
-                if ((key & 0xFFFFFFFFull) != (sl.last[k] & 0xFFFFFFFFull)) flags |= kStatusSeedTie;
-                const uint32_t tp = (tracklet_ptr + rank) % kTrackletRing;
-                tracklets[3 * tp] = static_cast<uint16_t>(sl.f0[k] + ((key >> 16) & 0xFFFFu));
-                tracklets[3 * tp + 1] = sl.h1[k];
-                tracklets[3 * tp + 2] = static_cast<uint16_t>(sl.f2[k] + (key & 0xFFFFu));
-                ttf[(ttf_ptr + rank) % kTtfModulo] = 0x80000000u | tp;
-              }
-              tracklet_ptr += nwin;
-              ttf_ptr += nwin;
-            }
-            __syncwarp();
           }
+          if (nc > 0 && (!have || nc + n_new > kSeedChunk)) flush();
+          if (!have) break;
+#pragma unroll
+          for (uint32_t j = 0; j < kSeedChunk / 32; ++j) {
+            const uint32_t h1 = start + r0 + 32 * j + lane;
+            const uint2 w = wv[j];
+            uint32_t cnt;
+            const uint32_t rank = ballot_rank(hv[j], cnt);
+            if (hv[j]) {
+              const uint32_t k = nc + rank;
+              const uint32_t f0 = w.x & 0xFFFFu, l0 = w.x >> 16, f2 = w.y & 0xFFFFu, l2 = w.y >> 16;
+              sl.h1[k] = static_cast<uint16_t>(h1);
+              sl.f0[k] = static_cast<uint16_t>(f0);
+              sl.np[k] = static_cast<uint16_t>(l0 - f0);
+              sl.f2[k] = static_cast<uint16_t>(f2);
+              sl.l2[k] = static_cast<uint16_t>(l2);
+              sl.best[k] = ~0ull;
+              sl.last[k] = 0ull;
+            }
+            nc += cnt;
+          }
+          n_h1 += n_new;
+          r0 += kSeedChunk;
         }
         if (n_h1 > kMaxHitsPerModule) flags |= kStatusH1Overflow;
         const uint32_t seeded = tracklet_ptr - tracklets_before;
