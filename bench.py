@@ -332,8 +332,10 @@ def run_ours(args, rank, world, local_rank):
         vc = vcs[0]
         # search mapping per hit-count bucket, tuned on the first batch (outside the timed region)
         threshold, tune_ms = autotune.tune_block_threshold(vc, *batch_ptrs[0], stream)
+        decode_warps, decode_ms = autotune.tune_decode_warps(vc, *batch_ptrs[0], stream)
         for other in vcs[1:]:
             other.set_block_threshold(threshold)
+            other.set_decode_warps(decode_warps)
         # census: per-batch totals for the algorithmic-byte accounting and the fallback share
         census = dict(clusters=0, tracks=0, track_hits=0, raw_bytes=raw_bytes, fallback_events=0)
         for raw_p, off_p, n in batch_ptrs:
@@ -357,7 +359,10 @@ def run_ours(args, rank, world, local_rank):
                        "roofline": roof, "census_per_step": census,
                        "search_mapping": {"block_above_clusters": threshold,
                                           "search_ms_per_threshold": {str(k): v for k, v in tune_ms.items()}},
-                       "gpu_launches": launches * n_batches * args.steps, "clocks": clocks, "threshold": threshold}
+                       "decode_block": {"warps": decode_warps,
+                                        "decode_ms_per_warps": {str(k): v for k, v in decode_ms.items()}},
+                       "gpu_launches": launches * n_batches * args.steps, "clocks": clocks, "threshold": threshold,
+                       "decode_warps": decode_warps}
         for v in vcs:
             v.close()
         log(f"[rank {rank}] {name}: {forms[name]['value']:.0f} events/s")
@@ -366,7 +371,8 @@ def run_ours(args, rank, world, local_rank):
     quality = run_quality(weights, args.quality_events, threads) if rank == 0 and args.quality_events > 0 else None
 
     # ---- end to end through velo_run_host with host buffers (pruned form) ----
-    e2e = run_e2e(args, chunks, plan, local_rank, torch, world, dist, forms["pruned"]["threshold"], weights)
+    e2e = run_e2e(args, chunks, plan, local_rank, torch, world, dist, forms["pruned"]["threshold"], weights,
+                   forms["pruned"]["decode_warps"])
 
     p, q = forms["pruned"], forms["plain"]
     result = {
@@ -379,6 +385,7 @@ def run_ours(args, rank, world, local_rank):
                    "batch_events": BUCKET, "batches_per_step": n_batches, "mode": "pruned", "graphs": True,
                    "streams": args.streams,
                    "scorer": scorer_info, "search_mapping": p["search_mapping"],
+                   "decode_block": p["decode_block"],
                    "l2": f"inputs larger than L2 ({raw_bytes / 1e9:.2f} GB raw banks per step)",
                    "parallelism": f"event shards x{world}"},
         "roofline": p["roofline"],
@@ -387,7 +394,8 @@ def run_ours(args, rank, world, local_rank):
         "fallback_fraction": p["census_per_step"]["fallback_events"] / n_events,
         "plain": {"value": q["value"], "ms_per_step": q["ms_per_step"], "stages_ms_per_step": q["stages_ms_per_step"],
                   "roofline": q["roofline"], "totals_per_step": q["census_per_step"], "clocks": q["clocks"],
-                  "search_mapping": q["search_mapping"], "gpu_launches": q["gpu_launches"]},
+                  "search_mapping": q["search_mapping"], "decode_block": q["decode_block"],
+                  "gpu_launches": q["gpu_launches"]},
         "pruned_vs_plain": p["value"] / q["value"],
         "quality": quality,
         "e2e": e2e,
@@ -397,7 +405,7 @@ def run_ours(args, rank, world, local_rank):
     return result, chunks
 
 
-def run_e2e(args, chunks, plan, local_rank, torch, world, dist, threshold, weights):
+def run_e2e(args, chunks, plan, local_rank, torch, world, dist, threshold, weights, decode_warps=8):
     """velo_run_host from pinned memory, E2E_CONTEXTS contexts in rotation, each on its own
     stream, so that the upload of one batch, the kernels of the next and the read-back of a
     third overlap (uploads and read-backs use the host link in opposite directions); outputs
@@ -416,6 +424,7 @@ def run_e2e(args, chunks, plan, local_rank, torch, world, dist, threshold, weigh
             for _ in range(nctx)]
     for vc in ctxs:
         vc.set_block_threshold(threshold)
+        vc.set_decode_warps(decode_warps)
         vc.set_mlp(weights)
         vc.set_mode(chain.MODE_PRUNED)
     streams = [torch.cuda.Stream(device=local_rank) for _ in range(nctx)]

@@ -129,6 +129,7 @@ GPU_SYMBOLS = [
     "velo_download",
     "velo_download_async",
     "velo_set_block_threshold",
+    "velo_set_decode_warps",
     "velo_last_launch_count",
     "velo_search_static",
     "velo_version",
@@ -219,6 +220,8 @@ def gpu_lib():
         lib.velo_download_async.restype = C.c_int
         lib.velo_set_block_threshold.argtypes = [P, C.c_uint32]
         lib.velo_set_block_threshold.restype = C.c_int
+        lib.velo_set_decode_warps.argtypes = [P, C.c_uint32]
+        lib.velo_set_decode_warps.restype = C.c_int
         lib.velo_last_launch_count.argtypes = [P, C.POINTER(C.c_uint32)]
         lib.velo_last_launch_count.restype = C.c_int
         lib.velo_search_static.argtypes = [P] * 4 + [C.c_uint32] + [P] * 5

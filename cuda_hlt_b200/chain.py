@@ -75,7 +75,7 @@ def decode_states(blob, T):
 
 class VeloChain:
     def __init__(self, max_events, max_raw_bytes, device=0, mode=MODE_PLAIN, mapping=MAP_AUTO, use_graphs=False,
-                 geometry=None, max_tracks=0, max_track_hits=0):
+                 geometry=None, max_tracks=0, max_track_hits=0, decode_warps=None):
         from . import events
         self.lib = _lib.gpu_lib()
         geometry = events.load_geometry() if geometry is None else geometry
@@ -87,6 +87,8 @@ class VeloChain:
                "velo_create")
         self.out = _lib.VeloOutputs()
         self.n_events = 0
+        if decode_warps is not None:
+            self.set_decode_warps(decode_warps)
 
     def close(self):
         if self.ctx:
@@ -146,6 +148,10 @@ class VeloChain:
     def set_block_threshold(self, clusters):
         """Events above `clusters` clusters use the block-per-event search, others the warp one."""
         _check(self.lib.velo_set_block_threshold(self.ctx, int(clusters)), "velo_set_block_threshold")
+
+    def set_decode_warps(self, warps):
+        """Decode block size: 4 or 8 warps per event."""
+        _check(self.lib.velo_set_decode_warps(self.ctx, int(warps)), "velo_set_decode_warps")
 
     def launch_count(self):
         n = C.c_uint32()

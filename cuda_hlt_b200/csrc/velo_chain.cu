@@ -277,6 +277,17 @@ int launch_chain(VeloCtx* c, const ChainPointers& P, cudaStream_t s, bool captur
   return 0;
 }
 
+// Persistent decode grid: as many blocks of the chosen size as are resident together.
+void size_decode_grid(VeloCtx* c)
+{
+  int occ = 0;
+  if (c->decode_warps == 8)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, decode_cluster_sort_kernel<8>, 256, 0);
+  else
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, decode_cluster_sort_kernel<4>, 128, 0);
+  c->decode_blocks = static_cast<uint32_t>(std::max(1, occ) * c->sm_count);
+}
+
 void drop_graphs(VeloCtx* c)
 {
   cudaSetDevice(c->device);
@@ -372,11 +383,7 @@ int velo_create(const VeloConfig* cfg, const void* geometry, size_t geometry_byt
       cudaMemcpy(c->d_sp_sizes, sizes, 256, cudaMemcpyHostToDevice) != cudaSuccess)
     return fail(VELO_ERR_CUDA);
   int occ = 0;
-  if (c->decode_warps == 8)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, decode_cluster_sort_kernel<8>, 256, 0);
-  else
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, decode_cluster_sort_kernel<4>, 128, 0);
-  c->decode_blocks = static_cast<uint32_t>(std::max(1, occ) * c->sm_count);
+  size_decode_grid(c);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, search_kernel<4>, 128, 0);
   c->search_blocks = static_cast<uint32_t>(std::max(1, occ) * c->sm_count);
   cudaFuncSetAttribute(search_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -644,6 +651,16 @@ int velo_download_async(VeloCtx* c, void* dst_host, const void* src_device, size
   if (cudaSetDevice(c->device) != cudaSuccess) return VELO_ERR_CUDA;
   VCK(cudaMemcpyAsync(dst_host, src_device, bytes, cudaMemcpyDeviceToHost, static_cast<cudaStream_t>(stream)));
   return 0;
+}
+
+int velo_set_decode_warps(VeloCtx* c, uint32_t warps)
+{
+  if (!c || (warps != 4 && warps != 8)) return VELO_ERR_INVALID;
+  if (cudaSetDevice(c->device) != cudaSuccess) return VELO_ERR_CUDA;
+  if (static_cast<int>(warps) != c->decode_warps) drop_graphs(c);  // the launch sequence changes
+  c->decode_warps = static_cast<int>(warps);
+  size_decode_grid(c);
+  return cudaGetLastError() == cudaSuccess ? 0 : VELO_ERR_CUDA;
 }
 
 int velo_set_block_threshold(VeloCtx* c, uint32_t clusters)

@@ -304,6 +304,10 @@ int velo_set_pv(VeloCtx* ctx, int enabled);
  * autotuner (cuda_hlt_b200/autotune.py) from timings per hit-count bucket. */
 int velo_set_block_threshold(VeloCtx* ctx, uint32_t clusters);
 
+/* Decode block size: 4 or 8 warps per event (default 8); set by the autotuner
+ * (cuda_hlt_b200/autotune.py) from decode timings on a sample batch. */
+int velo_set_decode_warps(VeloCtx* ctx, uint32_t warps);
+
 /* Kernel launch count of the last run (all kernels of this library). */
 int velo_last_launch_count(VeloCtx* ctx, uint32_t* n);
 

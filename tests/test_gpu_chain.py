@@ -250,6 +250,24 @@ def test_search_mappings_bit_exact(mapping):
         assert_states_equal(res, e, mt, g, gt, int(g["atomics"][N + e]), (mapping, e))
 
 
+@pytest.mark.parametrize("which", ["minbias", "batched"])
+def test_decode_block_sizes_bit_exact(which):
+    """Both decode block sizes the autotuner chooses between (4 and 8 warps per event) give the
+    reference's clusters and tracks."""
+    g = load_golden(which)
+    b = golden_batch(which)
+    res = run_chain(b, decode_warps=4)
+    N = b.n_events
+    for e in range(N):
+        if res["status"][e] & chain.REFERENCE_UNDEFINED:
+            continue
+        assert_clusters_equal(chain.event_clusters(res, e), golden_event_clusters(g, e), (which, e))
+        mt, gt = chain.event_tracks(res, e), golden_event_tracks(g, e)
+        assert pu.canonical_tracks(mt) == pu.canonical_tracks(gt), (which, e)
+    with pytest.raises(RuntimeError):
+        run_chain(b, decode_warps=6)
+
+
 def test_mappings_identical_on_uneven_batch():
     b = events.generate_config("batched_500k", n_events=400, first_event=3000)
     outs = [run_chain(b, mapping=m) for m in (chain.MAP_WARP, chain.MAP_BLOCK, chain.MAP_AUTO)]
