@@ -585,6 +585,74 @@ def pv_leg(batch, threshold):
     return out
 
 
+# Algorithmic bytes of the global event cut per event: the SciFi and UT bank offset tables,
+# the hit-count word of each UT bank, and the outputs (two counts, a flag, a list entry).
+def gec_bytes(ut, sf):
+    nu = ut.raw[ut.offsets[:-1].astype(np.int64)[:, None] + np.arange(4)].copy().view(np.uint32).ravel()
+    ns = sf.raw[sf.offsets[:-1].astype(np.int64)[:, None] + np.arange(4)].copy().view(np.uint32).ravel()
+    return int(np.sum(4 * (ns.astype(np.int64) + 2) + 4 * (nu.astype(np.int64) + 2) + 4 * nu.astype(np.int64) + 13))
+
+
+def gec_leg(batch, threshold, decode_warps):
+    """The global event cut in front of the plain chain on one batch (synthetic UT and SciFi
+    events of the same events, device-resident, graphs, CUDA events per stage), next to the
+    chain without the cut and to the reference's own kernel (oracle/_ref) on the same input."""
+    import torch
+    ut, sf = events.generate_ut_scifi(batch, seed=0)
+    dev = [torch.from_numpy(a).cuda() for a in (batch.raw, batch.offsets.view(np.int64), ut.raw,
+                                                 ut.offsets.view(np.int64), sf.raw, sf.offsets.view(np.int64))]
+    p = [t.data_ptr() for t in dev]
+    s = torch.cuda.current_stream().cuda_stream
+    n = batch.n_events
+    out = {"events": n, "ut_bytes_per_event": ut.raw.size / n, "scifi_bytes_per_event": sf.raw.size / n,
+           "timing": "CUDA events around the stage, single stream, mean of 5 runs"}
+    for name in ("with_cut", "without_cut"):
+        vc = chain.VeloChain(max_events=n, max_raw_bytes=int(batch.raw.size) + 4096, use_graphs=True)
+        vc.set_block_threshold(threshold)
+        vc.set_decode_warps(decode_warps)
+        vc.set_timing(True)
+
+        def once():
+            if name == "with_cut":
+                vc.run_gec_device(p[0], p[1], p[2], p[3], p[4], p[5], n, stream=s)
+            else:
+                vc.run_device(p[0], p[1], n, s)
+        for _ in range(2):
+            once()
+        torch.cuda.synchronize()
+        vc.set_timing(True)
+        for _ in range(5):
+            once()
+        t, _, _ = vc.sync(clusters=False)
+        st = vc.stage_times()
+        res = vc.results(clusters=False) if name == "with_cut" else None
+        vc.close()
+        runs = max(1, st.pop("runs"))
+        chain_ms = sum(st.values()) / runs
+        out[name] = {"chain_ms": chain_ms, "events_per_s": n / (chain_ms / 1e3), "tracks": t}
+        if res is not None:
+            gec_ms = st["global_event_cut"] / runs
+            b = gec_bytes(ut, sf)
+            out["selected"] = res["n_selected"]
+            out["gec_stage_ms"] = gec_ms
+            out["gec_events_per_s"] = n / (gec_ms / 1e3)
+            out["gec_algorithmic_bytes_per_event"] = b / n
+            out["gec_achieved_gbs"] = b / (gec_ms / 1e3) / 1e9
+    try:
+        import oracle
+        from oracle import gec_oracle
+        if os.path.exists(oracle.REF_GPU_LIB):
+            counts, _, _ = gec_oracle.run(ut, sf)
+            if np.all(counts[:, 1] < gec_oracle.MAX_CLUSTERS):  # see ref_harness.cu
+                sel, ms = oracle.ref_gec_run(ut, sf, reps=5, timed=True)
+                out["reference_kernel_ms"] = ms
+                out["reference_kernel_events_per_s"] = n / (ms / 1e3)
+                out["reference_selected"] = int(sel.size)
+    except Exception as ex:
+        out["reference_error"] = str(ex)
+    return out
+
+
 # ---------------------------------------------------------------------------
 # reference arm: the CPU implementation on the host cores
 # ---------------------------------------------------------------------------
@@ -669,6 +737,12 @@ def main():
                                       result["config"]["search_mapping"]["block_above_clusters"])
             except Exception as ex:
                 result["pv"] = {"error": str(ex)}
+            try:
+                result["global_event_cut"] = gec_leg(chunks[0].subset(0, min(SIDE_BATCH, chunks[0].n_events)),
+                                                     result["config"]["search_mapping"]["block_above_clusters"],
+                                                     result["config"]["decode_block"]["warps"])
+            except Exception as ex:
+                result["global_event_cut"] = {"error": str(ex)}
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

@@ -97,6 +97,20 @@ class VeloOutputs(C.Structure):
         ("pv_count", C.c_void_p),
         ("pv_zpeaks", C.c_void_p),
         ("pv_npeaks", C.c_void_p),
+        ("event_list", C.c_void_p),
+        ("n_selected", C.c_void_p),
+        ("gec_counts", C.c_void_p),
+        ("gec_flags", C.c_void_p),
+    ]
+
+
+class VeloGecInput(C.Structure):
+    _fields_ = [
+        ("ut_raw", C.c_void_p),
+        ("ut_offsets", C.c_void_p),
+        ("scifi_raw", C.c_void_p),
+        ("scifi_offsets", C.c_void_p),
+        ("max_clusters", C.c_uint32),
     ]
 
 
@@ -112,6 +126,7 @@ HOST_SYMBOLS = [
     "velo_gen_destroy",
     "velo_check_tracks",
     "velo_mdf_read",
+    "velo_mdf_read_banks",
     "velo_mdf_count",
     "velo_mdf_raw_bytes",
     "velo_mdf_copy",
@@ -121,6 +136,8 @@ GPU_SYMBOLS = [
     "velo_create",
     "velo_run",
     "velo_run_host",
+    "velo_run_gec",
+    "velo_run_gec_host",
     "velo_sync",
     "velo_set_mlp",
     "velo_stage_times",
@@ -178,6 +195,8 @@ def host_lib():
         lib.velo_check_tracks.restype = C.c_int
         lib.velo_mdf_read.argtypes = [C.c_char_p, C.c_uint64, C.c_uint64, C.POINTER(P)]
         lib.velo_mdf_read.restype = C.c_int
+        lib.velo_mdf_read_banks.argtypes = [C.c_char_p, C.c_uint64, C.c_uint64, C.c_uint32, C.POINTER(P)]
+        lib.velo_mdf_read_banks.restype = C.c_int
         lib.velo_mdf_count.argtypes = [P]
         lib.velo_mdf_count.restype = C.c_uint64
         lib.velo_mdf_raw_bytes.argtypes = [P]
@@ -204,6 +223,10 @@ def gpu_lib():
         lib.velo_run.restype = C.c_int
         lib.velo_run_host.argtypes = [P, P, P, C.c_uint32, P, C.POINTER(VeloOutputs)]
         lib.velo_run_host.restype = C.c_int
+        lib.velo_run_gec.argtypes = [P, P, P, C.POINTER(VeloGecInput), C.c_uint32, P, C.POINTER(VeloOutputs)]
+        lib.velo_run_gec.restype = C.c_int
+        lib.velo_run_gec_host.argtypes = [P, P, P, C.POINTER(VeloGecInput), C.c_uint32, P, C.POINTER(VeloOutputs)]
+        lib.velo_run_gec_host.restype = C.c_int
         lib.velo_sync.argtypes = [P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]
         lib.velo_sync.restype = C.c_int
         lib.velo_set_mlp.argtypes = [P, P, C.c_size_t]

@@ -31,7 +31,8 @@ SEQUENCE = (
     "velo_kalman_fit_t",
 )
 
-STAGES = ("decode_cluster_sort", "fill_candidates", "search_by_triplet", "event_scan", "consolidate_fit", "pv_beamline")
+STAGES = ("decode_cluster_sort", "fill_candidates", "search_by_triplet", "event_scan", "consolidate_fit", "pv_beamline",
+          "global_event_cut")
 PV_MAX_VERTICES = 32
 # VeloPvVertex (PV::Vertex layout)
 PV_VERTEX = np.dtype([("x", "<f4"), ("y", "<f4"), ("z", "<f4"), ("chi2", "<f4"), ("ndof", "<i4"), ("n_tracks", "<u4"),
@@ -46,8 +47,10 @@ STATUS = {
     "bad_raw": 1 << 0, "module_overflow": 1 << 1, "hit_overflow": 1 << 2, "candidate_overflow": 1 << 3,
     "track_overflow": 1 << 4, "ttf_overflow": 1 << 5, "weak_overflow": 1 << 6, "h1_overflow": 1 << 7,
     "big_sp_index": 1 << 8, "mlp_fallback": 1 << 9, "empty_module_read": 1 << 10, "seed_tie": 1 << 11,
-    "block_stage_timeout": 1 << 12, "pv_overflow": 1 << 13,
+    "block_stage_timeout": 1 << 12, "pv_overflow": 1 << 13, "not_selected": 1 << 14,
 }
+GEC_MAX_CLUSTERS = 9750  # maxSciFiUTClusters (cuda/global_event_cut/include/GlobalEventCut.cuh:9)
+GEC_PASS, GEC_MALFORMED = 1, 2
 # Flags of events whose reference result depends on unchecked buffer spills, reads outside
 # a module or the order of atomics (exact float ties).
 REFERENCE_UNDEFINED = sum(STATUS[k] for k in ("module_overflow", "candidate_overflow", "track_overflow",
@@ -113,6 +116,26 @@ class VeloChain:
         self.n_events = n_events
         _check(self.lib.velo_run(self.ctx, C.c_void_p(raw_ptr), C.c_void_p(offsets_ptr), n_events,
                                  C.c_void_p(stream), C.byref(self.out)), "velo_run")
+
+    def run_gec_host(self, batch, ut, scifi, max_clusters=GEC_MAX_CLUSTERS, stream=0):
+        """Global event cut on the UT and SciFi batches (EventBatch of the same events), then
+        the chain on the selected events: positions 0 .. n_selected - 1 hold raw events
+        event_list[0 ..] (results() adds both)."""
+        if not (batch.n_events == ut.n_events == scifi.n_events):
+            raise VeloError("VP, UT and SciFi batches must hold the same events")
+        self.n_events = batch.n_events
+        g = _lib.VeloGecInput(ut.raw.ctypes.data, ut.offsets.ctypes.data, scifi.raw.ctypes.data,
+                              scifi.offsets.ctypes.data, int(max_clusters))
+        _check(self.lib.velo_run_gec_host(self.ctx, batch.raw.ctypes.data, batch.offsets.ctypes.data, C.byref(g),
+                                          batch.n_events, C.c_void_p(stream), C.byref(self.out)), "velo_run_gec_host")
+
+    def run_gec_device(self, raw_ptr, offsets_ptr, ut_ptr, ut_offsets_ptr, scifi_ptr, scifi_offsets_ptr, n_events,
+                       max_clusters=GEC_MAX_CLUSTERS, stream=0):
+        """Same on device-resident inputs (u64 offsets[n+1] for each detector)."""
+        self.n_events = n_events
+        g = _lib.VeloGecInput(ut_ptr, ut_offsets_ptr, scifi_ptr, scifi_offsets_ptr, int(max_clusters))
+        _check(self.lib.velo_run_gec(self.ctx, C.c_void_p(raw_ptr), C.c_void_p(offsets_ptr), C.byref(g), n_events,
+                                     C.c_void_p(stream), C.byref(self.out)), "velo_run_gec")
 
     def sync(self, clusters=True):
         """Waits for the last run; returns (tracks, track hits, clusters or None)."""
@@ -189,6 +212,11 @@ class VeloChain:
             res["pv_count"] = self._down(o.pv_count, np.uint32, N)
             res["pv_zpeaks"] = self._down(o.pv_zpeaks, np.float32, N * M).reshape(N, M)
             res["pv_npeaks"] = self._down(o.pv_npeaks, np.uint32, N)
+        if o.event_list:
+            res["n_selected"] = int(self._down(o.n_selected, np.uint32, 1)[0])
+            res["event_list"] = self._down(o.event_list, np.uint32, N)[:res["n_selected"]]
+            res["gec_counts"] = self._down(o.gec_counts, np.uint32, 2 * N).reshape(N, 2)
+            res["gec_flags"] = self._down(o.gec_flags, np.uint8, N)
         if clusters:
             res["module_start"] = self._down(o.module_hit_start, np.uint32, N * N_MODULES)
             res["module_num"] = self._down(o.module_hit_num, np.uint32, N * N_MODULES)

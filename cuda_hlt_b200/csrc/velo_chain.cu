@@ -7,6 +7,7 @@
 #include <cstring>
 #include <array>
 #include <map>
+#include <tuple>
 #include <vector>
 
 #include "../../include/velo_b200.h"
@@ -20,6 +21,7 @@
 #include "velo_search_block.cuh"
 #include "velo_consolidate.cuh"
 #include "velo_pv.cuh"
+#include "velo_gec.cuh"
 
 // ============================================================================
 // C-ABI context
@@ -74,6 +76,14 @@ struct VeloCtx {
   PvVertex* d_pv_vertices = nullptr;
   uint32_t *d_pv_count = nullptr, *d_pv_npeaks = nullptr;
   float* d_pv_zpeaks = nullptr;
+  // global event cut (velo_run_gec): per-event counts and flags, the selected list, and the
+  // UT / SciFi staging of velo_run_gec_host (grown on demand)
+  uint32_t *d_gec_counts = nullptr, *d_event_list = nullptr, *d_n_selected = nullptr;
+  uint8_t* d_gec_flags = nullptr;
+  uint8_t *d_gec_ut = nullptr, *d_gec_scifi = nullptr;
+  uint64_t *d_gec_ut_offsets = nullptr, *d_gec_scifi_offsets = nullptr;
+  size_t gec_ut_cap = 0, gec_scifi_cap = 0;
+  uint32_t gec_blocks = 0;
   uint32_t* h_totals = nullptr;  // pinned [4]
   cudaStream_t last_stream = nullptr;
   uint32_t last_n = 0;
@@ -81,7 +91,9 @@ struct VeloCtx {
   bool timing = false;
   // Stage timing: one set of kStageEvents events per launch sequence; a graph keeps the set
   // it was captured with, plain launches cycle through the sets.
-  static constexpr int kStageEvents = 7;
+  // Events 0..6 bound the six chain stages in order; 7 and 8 bound the global event cut
+  // (recorded back to back when it does not run).
+  static constexpr int kStageEvents = 9;
   std::vector<std::array<cudaEvent_t, kStageEvents>> ev_sets;
   std::vector<uint8_t> ev_used;
   uint32_t ev_next = 0;
@@ -90,18 +102,21 @@ struct VeloCtx {
   int search_wpb = 4;
   uint32_t decode_blocks = 0, search_blocks = 0, search_block_blocks = 0, fill_blocks = 0, fill_pruned_blocks = 0,
            feature_blocks = 0, score_blocks = 0;
-  // CUDA graphs per (n_events, raw, offsets)
+  // CUDA graphs per (n_events, raw, offsets, stream, global event cut inputs)
   struct GraphKey {
     uint32_t n;
     const void* raw;
     const void* offsets;
     cudaStream_t stream;
+    const void* ut = nullptr;
+    const void* ut_offsets = nullptr;
+    const void* scifi = nullptr;
+    const void* scifi_offsets = nullptr;
+    uint32_t gec_max = 0;
     bool operator<(const GraphKey& o) const
     {
-      if (n != o.n) return n < o.n;
-      if (raw != o.raw) return raw < o.raw;
-      if (offsets != o.offsets) return offsets < o.offsets;
-      return stream < o.stream;
+      return std::tie(n, raw, offsets, stream, ut, ut_offsets, scifi, scifi_offsets, gec_max) <
+             std::tie(o.n, o.raw, o.offsets, o.stream, o.ut, o.ut_offsets, o.scifi, o.scifi_offsets, o.gec_max);
     }
   };
   struct GraphEntry {
@@ -140,7 +155,9 @@ void free_all(VeloCtx* c)
                   c->d_event_tracks, c->d_event_track_hits, c->d_atomics, c->d_track_hit_number,
                   c->d_event_hit_offset, c->d_track_hits_out, c->d_states, c->d_kalman, c->d_queue,
                   c->d_warp_events, c->d_block_events, c->d_event_order, c->d_pv_tracks, c->d_pv_vertices,
-                  c->d_pv_count, c->d_pv_npeaks, c->d_pv_zpeaks};
+                  c->d_pv_count, c->d_pv_npeaks, c->d_pv_zpeaks, c->d_gec_counts, c->d_event_list,
+                  c->d_n_selected, c->d_gec_flags, c->d_gec_ut, c->d_gec_scifi, c->d_gec_ut_offsets,
+                  c->d_gec_scifi_offsets};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c->h_totals) cudaFreeHost(c->h_totals);
@@ -212,11 +229,21 @@ cudaError_t record(cudaEvent_t e, cudaStream_t s, bool capturing)
   return capturing ? cudaEventRecordWithFlags(e, s, cudaEventRecordExternal) : cudaEventRecord(e, s);
 }
 
-int launch_chain(VeloCtx* c, const ChainPointers& P, cudaStream_t s, bool capturing = false)
+int launch_chain(VeloCtx* c, const ChainPointers& P, const GecPointers* G, cudaStream_t s, bool capturing = false)
 {
   const uint32_t n = P.n_events;
   c->launches = 0;
   VCK(cudaMemsetAsync(c->d_queue, 0, 8 * sizeof(uint32_t), s));
+  if (c->timing && c->ev_current >= 0) VCK(record(c->ev_sets[c->ev_current][7], s, capturing));
+  if (G) {  // global event cut: the event list decode reads
+    const uint32_t blocks = std::min<uint32_t>((n + kGecThreads / 32 - 1) / (kGecThreads / 32), c->gec_blocks);
+    gec_count_kernel<<<blocks, kGecThreads, 0, s>>>(*G);
+    VCK(cudaGetLastError());
+    gec_list_kernel<<<1, kGecListThreads, 0, s>>>(*G);
+    VCK(cudaGetLastError());
+    c->launches += 2;
+  }
+  if (c->timing && c->ev_current >= 0) VCK(record(c->ev_sets[c->ev_current][8], s, capturing));
   if (c->timing && c->ev_current >= 0) VCK(record(c->ev_sets[c->ev_current][0], s, capturing));
   {
     const uint32_t blocks = std::min<uint32_t>(n, c->decode_blocks);
@@ -367,6 +394,12 @@ int velo_create(const VeloConfig* cfg, const void* geometry, size_t geometry_byt
   ok &= dalloc(c->d_pv_zpeaks, static_cast<size_t>(N) * kPvMaxVertices) == cudaSuccess;
   ok &= dalloc(c->d_pv_count, N) == cudaSuccess;
   ok &= dalloc(c->d_pv_npeaks, N) == cudaSuccess;
+  ok &= dalloc(c->d_gec_counts, 2 * static_cast<size_t>(N)) == cudaSuccess;
+  ok &= dalloc(c->d_gec_flags, N) == cudaSuccess;
+  ok &= dalloc(c->d_event_list, N) == cudaSuccess;
+  ok &= dalloc(c->d_n_selected, 1) == cudaSuccess;
+  ok &= dalloc(c->d_gec_ut_offsets, static_cast<size_t>(N) + 1) == cudaSuccess;
+  ok &= dalloc(c->d_gec_scifi_offsets, static_cast<size_t>(N) + 1) == cudaSuccess;
   ok &= dalloc(c->d_queue, 8) == cudaSuccess;
   ok &= dalloc(c->d_warp_events, N) == cudaSuccess;
   ok &= dalloc(c->d_block_events, N) == cudaSuccess;
@@ -386,6 +419,8 @@ int velo_create(const VeloConfig* cfg, const void* geometry, size_t geometry_byt
   size_decode_grid(c);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, search_kernel<4>, 128, 0);
   c->search_blocks = static_cast<uint32_t>(std::max(1, occ) * c->sm_count);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, gec_count_kernel, kGecThreads, 0);
+  c->gec_blocks = static_cast<uint32_t>(std::max(1, occ) * c->sm_count);
   cudaFuncSetAttribute(search_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        static_cast<int>(kStageCap * sizeof(float4)));
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, search_block_kernel, kBlockThreads, kStageCap * sizeof(float4));
@@ -440,10 +475,13 @@ static int fill_outputs(VeloCtx* c, uint32_t n, VeloOutputs* out)
   return 0;
 }
 
-int velo_run(VeloCtx* c, const void* raw, const uint64_t* raw_offsets, uint32_t n_events, void* stream,
-             VeloOutputs* out)
+// velo_run with or without the global event cut in front (gec: device inputs, or null).
+static int run_chain(VeloCtx* c, const void* raw, const uint64_t* raw_offsets, const VeloGecInput* gec,
+                     uint32_t n_events, void* stream, VeloOutputs* out)
 {
   if (!c || (!raw && n_events) || (!raw_offsets && n_events)) return VELO_ERR_INVALID;
+  if (gec && n_events && (!gec->ut_raw || !gec->ut_offsets || !gec->scifi_raw || !gec->scifi_offsets))
+    return VELO_ERR_INVALID;
   if (n_events > c->cfg.max_events) return VELO_ERR_CAPACITY;
   if (c->mode == VELO_MODE_PRUNED && !c->mlp_loaded) return VELO_ERR_STATE;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -451,15 +489,38 @@ int velo_run(VeloCtx* c, const void* raw, const uint64_t* raw_offsets, uint32_t 
   c->last_stream = s;
   c->last_n = n_events;
   fill_outputs(c, n_events, out);
+  if (gec && out) {
+    out->event_list = c->d_event_list;
+    out->n_selected = c->d_n_selected;
+    out->gec_counts = c->d_gec_counts;
+    out->gec_flags = c->d_gec_flags;
+  }
   if (n_events == 0) {
     VCK(cudaMemsetAsync(c->d_atomics, 0, sizeof(uint32_t), s));
     VCK(cudaMemsetAsync(c->d_track_hit_number, 0, sizeof(uint32_t), s));
     VCK(cudaMemsetAsync(c->d_event_hit_offset, 0, sizeof(uint32_t), s));
+    if (gec) VCK(cudaMemsetAsync(c->d_n_selected, 0, sizeof(uint32_t), s));
     return 0;
   }
-  const ChainPointers P = pointers(c, raw, raw_offsets, n_events);
+  ChainPointers P = pointers(c, raw, raw_offsets, n_events);
+  GecPointers G{};
+  if (gec) {
+    G = GecPointers{static_cast<const uint8_t*>(gec->ut_raw), gec->ut_offsets,
+                    static_cast<const uint8_t*>(gec->scifi_raw), gec->scifi_offsets, n_events, gec->max_clusters,
+                    c->d_gec_counts, c->d_gec_flags, c->d_event_list, c->d_n_selected};
+    P.event_list = c->d_event_list;
+    P.n_selected = c->d_n_selected;
+  }
+  const GecPointers* Gp = gec ? &G : nullptr;
   if (c->cfg.use_graphs) {
-    const VeloCtx::GraphKey key{n_events, raw, raw_offsets, s};
+    VeloCtx::GraphKey key{n_events, raw, raw_offsets, s};
+    if (gec) {
+      key.ut = gec->ut_raw;
+      key.ut_offsets = gec->ut_offsets;
+      key.scifi = gec->scifi_raw;
+      key.scifi_offsets = gec->scifi_offsets;
+      key.gec_max = gec->max_clusters;
+    }
     auto it = c->graphs.find(key);
     if (it == c->graphs.end()) {
       cudaStream_t cap = s;
@@ -477,7 +538,7 @@ int velo_run(VeloCtx* c, const void* raw, const uint64_t* raw_offsets, uint32_t 
       c->ev_current = set;
       cudaGraph_t g;
       VCK(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
-      const int rc = launch_chain(c, P, cap, true);
+      const int rc = launch_chain(c, P, Gp, cap, true);
       cudaError_t ce = cudaStreamEndCapture(cap, &g);
       if (tmp) cudaStreamDestroy(cap);
       if (rc != 0) return rc;
@@ -497,7 +558,78 @@ int velo_run(VeloCtx* c, const void* raw, const uint64_t* raw_offsets, uint32_t 
     c->ev_current = static_cast<int>(c->ev_next++ % kPlainEventSets);
     c->ev_used[c->ev_current] = 1;
   }
-  return launch_chain(c, P, s);
+  return launch_chain(c, P, Gp, s);
+}
+
+int velo_run(VeloCtx* c, const void* raw, const uint64_t* raw_offsets, uint32_t n_events, void* stream,
+             VeloOutputs* out)
+{
+  return run_chain(c, raw, raw_offsets, nullptr, n_events, stream, out);
+}
+
+int velo_run_gec(VeloCtx* c, const void* raw, const uint64_t* raw_offsets, const VeloGecInput* gec,
+                 uint32_t n_events, void* stream, VeloOutputs* out)
+{
+  if (!gec) return VELO_ERR_INVALID;
+  return run_chain(c, raw, raw_offsets, gec, n_events, stream, out);
+}
+
+// Copies a host batch (bytes from offsets[0] to offsets[n], offsets[n + 1]) to device buffers,
+// rebasing the offsets when the batch does not start at byte 0.
+static int upload_batch(const void* raw_host, const uint64_t* offsets_host, uint32_t n, uint8_t* d_raw,
+                        uint64_t* d_offsets, cudaStream_t s)
+{
+  const uint64_t first = offsets_host[0];
+  const uint64_t bytes = offsets_host[n] - first;
+  VCK(cudaMemcpyAsync(d_raw, static_cast<const uint8_t*>(raw_host) + first, bytes, cudaMemcpyHostToDevice, s));
+  if (first == 0) {
+    VCK(cudaMemcpyAsync(d_offsets, offsets_host, 8ull * (n + 1), cudaMemcpyHostToDevice, s));
+  } else {
+    std::vector<uint64_t> rebased(offsets_host, offsets_host + n + 1);
+    for (auto& v : rebased) v -= first;
+    VCK(cudaMemcpyAsync(d_offsets, rebased.data(), 8ull * (n + 1), cudaMemcpyHostToDevice, s));
+    VCK(cudaStreamSynchronize(s));
+  }
+  return 0;
+}
+
+// Grows a staging buffer to hold `bytes` (the graphs that recorded the old address go).
+static int ensure_staging(VeloCtx* c, uint8_t*& p, size_t& cap, uint64_t bytes)
+{
+  if (bytes <= cap && p) return 0;
+  drop_graphs(c);
+  if (p) cudaFree(p);
+  p = nullptr;
+  cap = 0;
+  const size_t want = std::max<size_t>(bytes + bytes / 4, 1 << 20);
+  VCK(cudaMalloc(reinterpret_cast<void**>(&p), want));
+  cap = want;
+  return 0;
+}
+
+int velo_run_gec_host(VeloCtx* c, const void* raw_host, const uint64_t* raw_offsets_host,
+                      const VeloGecInput* gec_host, uint32_t n_events, void* stream, VeloOutputs* out)
+{
+  if (!c || !raw_host || !raw_offsets_host || !gec_host || !gec_host->ut_raw || !gec_host->ut_offsets ||
+      !gec_host->scifi_raw || !gec_host->scifi_offsets)
+    return VELO_ERR_INVALID;
+  if (n_events > c->cfg.max_events) return VELO_ERR_CAPACITY;
+  if (raw_offsets_host[n_events] - raw_offsets_host[0] > c->cfg.max_raw_bytes) return VELO_ERR_CAPACITY;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (cudaSetDevice(c->device) != cudaSuccess) return VELO_ERR_CUDA;
+  const uint64_t ut_bytes = gec_host->ut_offsets[n_events] - gec_host->ut_offsets[0];
+  const uint64_t scifi_bytes = gec_host->scifi_offsets[n_events] - gec_host->scifi_offsets[0];
+  int rc = ensure_staging(c, c->d_gec_ut, c->gec_ut_cap, ut_bytes);
+  if (rc == 0) rc = ensure_staging(c, c->d_gec_scifi, c->gec_scifi_cap, scifi_bytes);
+  if (rc == 0) rc = upload_batch(raw_host, raw_offsets_host, n_events, c->d_raw, c->d_raw_offsets, s);
+  if (rc == 0) rc = upload_batch(gec_host->ut_raw, gec_host->ut_offsets, n_events, c->d_gec_ut, c->d_gec_ut_offsets, s);
+  if (rc == 0)
+    rc = upload_batch(gec_host->scifi_raw, gec_host->scifi_offsets, n_events, c->d_gec_scifi,
+                      c->d_gec_scifi_offsets, s);
+  if (rc) return rc;
+  const VeloGecInput dev{c->d_gec_ut, c->d_gec_ut_offsets, c->d_gec_scifi, c->d_gec_scifi_offsets,
+                         gec_host->max_clusters};
+  return run_chain(c, c->d_raw, c->d_raw_offsets, &dev, n_events, stream, out);
 }
 
 int velo_run_host(VeloCtx* c, const void* raw_host, const uint64_t* raw_offsets_host, uint32_t n_events, void* stream,
@@ -505,21 +637,11 @@ int velo_run_host(VeloCtx* c, const void* raw_host, const uint64_t* raw_offsets_
 {
   if (!c || !raw_host || !raw_offsets_host) return VELO_ERR_INVALID;
   if (n_events > c->cfg.max_events) return VELO_ERR_CAPACITY;
-  const uint64_t first = raw_offsets_host[0];
-  const uint64_t bytes = raw_offsets_host[n_events] - first;
-  if (bytes > c->cfg.max_raw_bytes) return VELO_ERR_CAPACITY;
+  if (raw_offsets_host[n_events] - raw_offsets_host[0] > c->cfg.max_raw_bytes) return VELO_ERR_CAPACITY;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (cudaSetDevice(c->device) != cudaSuccess) return VELO_ERR_CUDA;
-  VCK(cudaMemcpyAsync(c->d_raw, static_cast<const uint8_t*>(raw_host) + first, bytes, cudaMemcpyHostToDevice, s));
-  if (first == 0) {
-    VCK(cudaMemcpyAsync(c->d_raw_offsets, raw_offsets_host, 8ull * (n_events + 1), cudaMemcpyHostToDevice, s));
-  } else {
-    // rebase the offsets on the host only when the caller passed a slice
-    std::vector<uint64_t> rebased(raw_offsets_host, raw_offsets_host + n_events + 1);
-    for (auto& v : rebased) v -= first;
-    VCK(cudaMemcpyAsync(c->d_raw_offsets, rebased.data(), 8ull * (n_events + 1), cudaMemcpyHostToDevice, s));
-    VCK(cudaStreamSynchronize(s));
-  }
+  const int rc = upload_batch(raw_host, raw_offsets_host, n_events, c->d_raw, c->d_raw_offsets, s);
+  if (rc) return rc;
   return velo_run(c, c->d_raw, c->d_raw_offsets, n_events, stream, out);
 }
 
@@ -616,7 +738,7 @@ int velo_set_timing(VeloCtx* c, int enabled)
 // number of launch sequences summed.
 int velo_stage_times(VeloCtx* c, float* ms, int n)
 {
-  constexpr int kStages = VeloCtx::kStageEvents - 1;
+  constexpr int kStages = 7;  // six chain stages and the global event cut
   if (!c || !ms || n < kStages) return VELO_ERR_INVALID;
   if (c->ev_sets.empty()) return VELO_ERR_STATE;
   float acc[kStages] = {};
@@ -625,7 +747,8 @@ int velo_stage_times(VeloCtx* c, float* ms, int n)
     if (!c->ev_used[k]) continue;
     for (int i = 0; i < kStages; ++i) {
       float t = 0.f;
-      VCK(cudaEventElapsedTime(&t, c->ev_sets[k][i], c->ev_sets[k][i + 1]));
+      const int a = i < kStages - 1 ? i : 7, b = i < kStages - 1 ? i + 1 : 8;
+      VCK(cudaEventElapsedTime(&t, c->ev_sets[k][a], c->ev_sets[k][b]));
       acc[i] += t;
     }
     ++runs;

@@ -346,8 +346,14 @@ __global__ void __launch_bounds__(W * 32, 40 / W) decode_cluster_sort_kernel(Cha
     __syncthreads();
     const uint32_t e = sh.event;
     if (e >= P.n_events) break;
-    const uint64_t off = P.raw_offsets[e];
-    const uint64_t bytes = P.raw_offsets[e + 1] - off;
+    uint32_t src = e;  // raw event of this position
+    bool skipped = false;
+    if (P.event_list) {
+      if (e < *P.n_selected) src = P.event_list[e];
+      else skipped = true;
+    }
+    const uint64_t off = skipped ? 0 : P.raw_offsets[src];
+    const uint64_t bytes = skipped ? 0 : P.raw_offsets[src + 1] - off;
     const uint32_t* ev = reinterpret_cast<const uint32_t*>(P.raw + off);
     const uint64_t words = bytes / 4;
     const uint32_t header = 2 + kSensors;  // number_of_raw_banks + raw_bank_offset[209]
@@ -376,10 +382,10 @@ __global__ void __launch_bounds__(W * 32, 40 / W) decode_cluster_sort_kernel(Cha
         if (count > 256) atomicOr(&sh.flags, kStatusBigSpIndex);
       }
     } else if (threadIdx.x == 0) {
-      atomicOr(&sh.flags, kStatusBadRawEvent);
+      atomicOr(&sh.flags, skipped ? kStatusNotSelected : kStatusBadRawEvent);
     }
     __syncthreads();
-    const bool event_ok = !(sh.flags & kStatusBadRawEvent);
+    const bool event_ok = !(sh.flags & (kStatusBadRawEvent | kStatusNotSelected));
     if (!event_ok)
       for (uint32_t b = threadIdx.x; b <= kSensors; b += blockDim.x) sh.sp_prefix[b] = 0;
     // ---- bank prefix (warp 0) ----

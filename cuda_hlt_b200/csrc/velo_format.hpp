@@ -126,6 +126,7 @@ enum StatusFlags : uint32_t {
   kStatusH1Overflow = 1u << 7,        // > kMaxHitsPerModule seeding h1 hits in one step
   kStatusBigSpIndex = 1u << 8,        // a bank holds > 256 SPs (reference u8 sp_index wraps)
   kStatusMlpFallback = 1u << 9,       // learned pruning skipped: occupancy outside trained range
+  kStatusNotSelected = 1u << 14,      // position beyond the events the global event cut selected
 };
 
 }  // namespace velo

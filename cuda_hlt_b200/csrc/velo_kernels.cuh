@@ -77,6 +77,10 @@ struct ChainPointers {
   const uint8_t* raw;
   const uint64_t* raw_offsets;  // [N+1]
   uint32_t n_events;
+  // global event cut (null without it): position e < *n_selected decodes raw event
+  // event_list[e]; later positions are left empty
+  const uint32_t* event_list;
+  const uint32_t* n_selected;
   DeviceConstants k;
   // clusters
   HitsAoS hits;

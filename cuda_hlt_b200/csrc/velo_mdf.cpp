@@ -1,6 +1,8 @@
-// MDF reader: the VP raw banks of the events of an LHCb MDF file, laid out as velo_run takes
-// them. Follows MDF::read_events / read_event / read_banks (mdf/src/read_mdf.cpp:29-313) for
-// BankTypes::VP, with the record format of mdf/include/mdf_header.hpp and
+// MDF reader: the raw banks of one type (VP by default; UT and FTCluster for the global event
+// cut) of the events of an LHCb MDF file, laid out as velo_run takes them. Follows
+// MDF::read_events / read_event / read_banks (mdf/src/read_mdf.cpp:29-313) with the bank types
+// of LHCbToGPU::bank_types (mdf/include/read_mdf.hpp:20-24), the record format of
+// mdf/include/mdf_header.hpp and
 // mdf/include/raw_bank.hpp, the checksum of LHCb::genChecksum (mdf/src/raw_helpers.cpp:8-21,
 // 186-199) and the ROOT-style zlib blocks of Compression::unzip (mdf/src/compression.cpp).
 //
@@ -10,8 +12,8 @@
 // ROOT blocks ("ZL", method 8, 3-byte compressed size, 3-byte expanded size, zlib stream)
 // when the compression byte's low nibble is non-zero. A raw bank is {magic 0xCBCB u16,
 // length u16 (with the 8-byte header), type u8, version u8, source id i16, body}, padded to
-// 4 bytes. Per event the output holds: number of VP banks, their byte offsets (one more
-// than banks) and for each bank its source id followed by its body words.
+// 4 bytes. Per event the output holds: number of banks of the type, their byte offsets (one
+// more than banks) and for each bank its source id followed by its body words.
 #include <zlib.h>
 
 #include <cstdint>
@@ -91,9 +93,10 @@ struct VeloMdfEvents {
   std::vector<uint64_t> event;       // ODIN event number per event (0 without ODIN)
 };
 
-extern "C" int velo_mdf_read(const char* path, uint64_t first_event, uint64_t max_events, VeloMdfEvents** out)
+extern "C" int velo_mdf_read_banks(const char* path, uint64_t first_event, uint64_t max_events, uint32_t bank_type,
+                                   VeloMdfEvents** out)
 {
-  if (!path || !out) return VELO_ERR_INVALID;
+  if (!path || !out || bank_type > 255 || bank_type == kBankODIN) return VELO_ERR_INVALID;
   *out = nullptr;
   FILE* f = std::fopen(path, "rb");
   if (!f) return VELO_ERR_INVALID;
@@ -133,7 +136,7 @@ extern "C" int velo_mdf_read(const char* path, uint64_t first_event, uint64_t ma
       body = banks.data();
       body_len = banks.size();
     }
-    // walk the banks: VP ones into the event, ODIN for the event identity
+    // walk the banks: those of the type into the event, ODIN for the event identity
     bank_words.clear();
     bank_offsets.assign(1, 0u);
     uint32_t run = 0;
@@ -160,7 +163,7 @@ extern "C" int velo_mdf_read(const char* path, uint64_t first_event, uint64_t ma
       if (type == kBankODIN && nwords >= 5) {
         run = rd32(b + 8);
         evno = (static_cast<uint64_t>(rd32(b + 8 + 3 * 4)) << 32) + rd32(b + 8 + 4 * 4);
-      } else if (type == kBankVP) {
+      } else if (type == bank_type) {
         bank_words.push_back(static_cast<uint32_t>(static_cast<int32_t>(source)));
         for (uint32_t w = 0; w < nwords; ++w) bank_words.push_back(rd32(b + 8 + 4 * w));
         bank_offsets.push_back(static_cast<uint32_t>(bank_words.size() * 4));
@@ -187,6 +190,11 @@ extern "C" int velo_mdf_read(const char* path, uint64_t first_event, uint64_t ma
   }
   *out = ev;
   return 0;
+}
+
+extern "C" int velo_mdf_read(const char* path, uint64_t first_event, uint64_t max_events, VeloMdfEvents** out)
+{
+  return velo_mdf_read_banks(path, first_event, max_events, kBankVP, out);
 }
 
 extern "C" uint64_t velo_mdf_count(const VeloMdfEvents* e) { return e ? e->run.size() : 0; }

@@ -121,20 +121,25 @@ def read_bank_folder(vp_folder, mc_folder=None, limit=None):
     return batch
 
 
-def read_mdf(path, first_event=0, max_events=None):
-    """VP raw banks of the events of an MDF file (velo_mdf_read, the counterpart of
-    MDF::read_events for BankTypes::VP) or of every *.mdf file of a folder in name order;
-    event names are "run_event" from the ODIN bank."""
+# LHCb raw bank type numbers (mdf/include/raw_bank.hpp) of the detectors the readers take
+BANK_TYPES = {"VP": 63, "FTCluster": 64, "UT": 66, "Muon": 13}
+
+
+def read_mdf(path, first_event=0, max_events=None, bank="VP"):
+    """Raw banks of one type (VP by default; "UT", "FTCluster", "Muon") of the events of an
+    MDF file (velo_mdf_read_banks, the counterpart of MDF::read_events) or of every *.mdf
+    file of a folder in name order; event names are "run_event" from the ODIN bank."""
     import ctypes as C
     lib = _lib.host_lib()
+    bank_type = BANK_TYPES[bank]
     files = sorted(glob.glob(os.path.join(path, "*.mdf"))) if os.path.isdir(path) else [path]
     raws, names, skip = [], [], first_event
     left = (1 << 62) if max_events is None else max_events
     for f in files:
         h = C.c_void_p()
-        rc = lib.velo_mdf_read(f.encode(), skip, left, C.byref(h))
+        rc = lib.velo_mdf_read_banks(f.encode(), skip, left, bank_type, C.byref(h))
         if rc != 0:
-            raise ValueError(f"velo_mdf_read({f}) failed with code {rc}")
+            raise ValueError(f"velo_mdf_read_banks({f}, {bank}) failed with code {rc}")
         try:
             n = lib.velo_mdf_count(h)
             raw = np.zeros(lib.velo_mdf_raw_bytes(h), np.uint8)
@@ -153,6 +158,50 @@ def read_mdf(path, first_event=0, max_events=None):
     offsets = np.zeros(len(raws) + 1, dtype=np.uint64)
     offsets[1:] = np.cumsum([r.size for r in raws])
     return EventBatch(np.concatenate(raws) if raws else np.zeros(0, np.uint8), offsets, names=names)
+
+
+# Synthetic UT and SciFi (FTCluster) raw events for the global event cut. Occupancy follows
+# the VELO event's: hits ~ Poisson(rate x VP raw words), with the rates of the ten minbias
+# events shipped with the reference (UT hits / VP words = 0.38, SciFi cluster estimate /
+# VP words = 1.41 over the ten). Bank counts are those of the same events: 180 UT banks,
+# 240 SciFi banks. UT bank: source id, a word whose low 16 bits hold the hit count, one
+# 32-bit word per hit (UTRaw.cuh; the minbias banks hold about 4 bytes per hit); SciFi bank:
+# source id, then 16-bit clusters padded to 4 bytes (SciFiRaw.cuh). Hit and cluster words are
+# random: the cut reads counts and sizes only.
+UT_BANKS, SCIFI_BANKS = 180, 240
+UT_PER_VP_WORD, SCIFI_PER_VP_WORD = 0.38, 1.41
+
+
+def _banks_to_raw(counts, header_words, items_per_word, rng):
+    """Raw events (u32 layout: number of banks, bank byte offsets [B + 1], banks) from a
+    [N, B] array of items per bank, `items_per_word` items to a 32-bit word; each bank starts
+    with `header_words` words, the source id and, with two header words, the item count."""
+    n, nb = counts.shape
+    words = header_words + (counts + items_per_word - 1) // items_per_word  # [N, B]
+    ev_words = 1 + (nb + 1) + words.sum(axis=1)                  # [N]
+    ev_start = np.zeros(n + 1, np.int64)
+    ev_start[1:] = np.cumsum(ev_words)
+    raw = rng.integers(0, 1 << 32, size=int(ev_start[-1]), dtype=np.uint64).astype(np.uint32)
+    bank_off = np.zeros((n, nb + 1), np.int64)                   # word offsets inside the payload
+    bank_off[:, 1:] = np.cumsum(words, axis=1)
+    raw[ev_start[:-1]] = nb
+    cols = np.arange(nb + 1)
+    raw[(ev_start[:-1, None] + 1 + cols[None, :]).ravel()] = (4 * bank_off).astype(np.uint32).ravel()
+    bank_at = ev_start[:-1, None] + 1 + (nb + 1) + bank_off[:, :-1]   # first word of each bank
+    raw[bank_at.ravel()] = np.tile(np.arange(nb, dtype=np.uint32), n)
+    if header_words == 2:
+        raw[(bank_at + 1).ravel()] = counts.astype(np.uint32).ravel()
+    offsets = (4 * ev_start).astype(np.uint64)
+    return EventBatch(raw.view(np.uint8), offsets)
+
+
+def generate_ut_scifi(vp_batch, seed=0):
+    """(UT batch, SciFi batch) for the events of `vp_batch`, seeded."""
+    rng = np.random.default_rng(seed)
+    vp_words = np.diff(vp_batch.offsets).astype(np.float64) / 4.0
+    ut = rng.poisson((UT_PER_VP_WORD * vp_words / UT_BANKS)[:, None], size=(vp_batch.n_events, UT_BANKS))
+    sf = rng.poisson((SCIFI_PER_VP_WORD * vp_words / SCIFI_BANKS)[:, None], size=(vp_batch.n_events, SCIFI_BANKS))
+    return _banks_to_raw(ut, 2, 1, rng), _banks_to_raw(sf, 1, 2, rng)
 
 
 def validate(batch):

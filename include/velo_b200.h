@@ -63,6 +63,8 @@ extern "C" {
 #define VELO_STATUS_MLP_FALLBACK (1u << 9)
 #define VELO_STATUS_PV_OVERFLOW (1u << 13) /* PV stage: peaks, clusters or extrema beyond the
                                               reference's fixed arrays (it writes past them) */
+#define VELO_STATUS_NOT_SELECTED (1u << 14) /* velo_run_gec: position at or beyond the number of
+                                               selected events (left empty) */
 
 /* ======================================================================
  * Host utilities (libvelo_host.so; no GPU needed)
@@ -129,6 +131,15 @@ int velo_check_tracks(const void* mc_blob, const uint64_t* mc_offsets, uint32_t 
  * reference prints and stops at the first such record, or, for a bad bank magic, goes on). */
 typedef struct VeloMdfEvents VeloMdfEvents;
 int velo_mdf_read(const char* path, uint64_t first_event, uint64_t max_events, VeloMdfEvents** out);
+/* Same for the banks of another LHCb raw bank type (LHCb::RawBank::BankType numbers,
+ * mdf/include/raw_bank.hpp: VP 63, FTCluster 64, UT 66, Muon 13), e.g. the UT and SciFi
+ * inputs of velo_run_gec; the layout per event is the same. */
+#define VELO_BANK_VP 63u
+#define VELO_BANK_FTCLUSTER 64u
+#define VELO_BANK_UT 66u
+#define VELO_BANK_MUON 13u
+int velo_mdf_read_banks(const char* path, uint64_t first_event, uint64_t max_events, uint32_t bank_type,
+                        VeloMdfEvents** out);
 uint64_t velo_mdf_count(const VeloMdfEvents* events);
 uint64_t velo_mdf_raw_bytes(const VeloMdfEvents* events);
 /* raw[raw_bytes], offsets[count + 1] (u64 byte offsets), run[count], event[count]; any may be null */
@@ -190,6 +201,14 @@ typedef struct VeloOutputs {
   uint32_t* pv_count;    /* [n_events] vertices of each event */
   float* pv_zpeaks;      /* [n_events * VELO_PV_MAX_VERTICES] z of the histogram peaks (seeds) */
   uint32_t* pv_npeaks;   /* [n_events] */
+  /* global event cut (velo_run_gec; null after velo_run). Positions 0 .. *n_selected - 1 of
+   * every per-event output above hold the selected raw events event_list[0 ..], in ascending
+   * order; later positions are empty (VELO_STATUS_NOT_SELECTED). */
+  uint32_t* event_list;  /* [n_events] dev_event_list */
+  uint32_t* n_selected;  /* [1] dev_number_of_selected_events */
+  uint32_t* gec_counts;  /* [2 * n_events] per raw event: SciFi cluster estimate, UT hits
+                            (0xFFFFFFFF: malformed bank table) */
+  uint8_t* gec_flags;    /* [n_events] per raw event: VELO_GEC_PASS | VELO_GEC_MALFORMED */
 } VeloOutputs;
 
 /* A primary vertex, in the layout of PV::Vertex (cuda/PV/beamlinePV/include/PV_Definitions.cuh:64-109). */
@@ -216,6 +235,32 @@ int velo_run(VeloCtx* ctx, const void* raw, const uint64_t* raw_offsets, uint32_
  * buffers on the stream, then runs. */
 int velo_run_host(VeloCtx* ctx, const void* raw_host, const uint64_t* raw_offsets_host, uint32_t n_events,
                   void* stream, VeloOutputs* out);
+
+/* Global event cut in front of the chain: global_event_cut_t
+ * (cuda/global_event_cut/src/GlobalEventCut.cu:3-55, configuration/sequences/Velo.h:7).
+ * An event passes when its SciFi cluster estimate, (sum over FTCluster banks of (bank bytes
+ * - 4)) / 2 - 2 in 32-bit unsigned arithmetic, is below max_clusters and that plus its UT
+ * hit count (sum over UT banks of the low 16 bits of the bank's second word) is below
+ * max_clusters too. UT and SciFi raw events have the layout of UTRaw.cuh / SciFiRaw.cuh:
+ * u32 number of banks, u32 bank byte offsets [banks + 1], the banks. The chain then runs on
+ * the selected events without a host synchronisation (the reference reads the selected
+ * count back before its next kernel). */
+#define VELO_GEC_MAX_CLUSTERS 9750u /* maxSciFiUTClusters, GlobalEventCut.cuh:9 */
+#define VELO_GEC_PASS 1u
+#define VELO_GEC_MALFORMED 2u       /* bank table or a UT bank header outside the event: fails */
+typedef struct VeloGecInput {
+  const void* ut_raw;             /* UT raw events, back to back */
+  const uint64_t* ut_offsets;     /* [n_events + 1] byte offsets */
+  const void* scifi_raw;          /* FTCluster raw events */
+  const uint64_t* scifi_offsets;  /* [n_events + 1] */
+  uint32_t max_clusters;          /* VELO_GEC_MAX_CLUSTERS */
+} VeloGecInput;
+/* Device inputs (all pointers device-resident). */
+int velo_run_gec(VeloCtx* ctx, const void* raw, const uint64_t* raw_offsets, const VeloGecInput* gec,
+                 uint32_t n_events, void* stream, VeloOutputs* out);
+/* Host inputs: copies the three detectors' batches to device buffers of the context first. */
+int velo_run_gec_host(VeloCtx* ctx, const void* raw_host, const uint64_t* raw_offsets_host,
+                      const VeloGecInput* gec_host, uint32_t n_events, void* stream, VeloOutputs* out);
 
 /* Waits for the context's last run; fills totals (tracks, track hits, clusters). */
 int velo_sync(VeloCtx* ctx, uint32_t* total_tracks, uint32_t* total_track_hits, uint64_t* total_clusters);
@@ -280,8 +325,8 @@ int velo_mlp_infer(VeloMlpTrainer* t, const float* features, uint32_t n, float* 
 
 /* Device time of each stage of the runs recorded since velo_set_timing, milliseconds:
  * ms[0] decode+cluster+sort, ms[1] fill_candidates (windows, scorer), ms[2] search,
- * ms[3] scan, ms[4] consolidate+fit, ms[5] beamline PV (0 when off), ms[6] (n > 6) number of
- * runs summed. */
+ * ms[3] scan, ms[4] consolidate+fit, ms[5] beamline PV (0 when off), ms[6] global event cut
+ * (0 without velo_run_gec), ms[7] (n > 7) number of runs summed. */
 int velo_stage_times(VeloCtx* ctx, float* ms, int n);
 int velo_set_timing(VeloCtx* ctx, int enabled);
 

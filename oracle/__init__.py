@@ -154,6 +154,8 @@ def ref_gpu_lib():
         L.ref_pv_vertex_size.restype = C.c_int
         L.ref_pv_run.argtypes = [P, P, P, C.c_uint32, P, P, P, P, P, C.c_int, C.POINTER(C.c_float)]
         L.ref_pv_run.restype = C.c_int
+        L.ref_gec_run.argtypes = [P, P, P, P, C.c_uint32, P, P, C.c_int, C.POINTER(C.c_float)]
+        L.ref_gec_run.restype = C.c_int
         _ref_gpu = L
     return _ref_gpu
 
@@ -225,6 +227,28 @@ def ref_pv_run(atomics, track_hit_number, kalman_raw, n_events, reps=1):
     out["vertex_size"] = vs
     out["ms"] = ms.value
     return out
+
+
+def ref_gec_run(ut_batch, scifi_batch, reps=1, timed=False):
+    """The reference's global_event_cut kernel (GlobalEventCut.cu:3-55) on UT and SciFi
+    batches (u32 offsets, as the reference takes them). Returns the selected events in the
+    kernel's order (an atomic counter's: unspecified), and with timed=True also the mean
+    device ms of one launch. Only for events whose UT hit total is below the cut (see
+    ref_harness.cu); the caller checks that with gec_oracle first."""
+    L = ref_gpu_lib()
+    N = ut_batch.n_events
+    ut_off = np.ascontiguousarray(ut_batch.offsets - ut_batch.offsets[0], np.uint32)
+    sf_off = np.ascontiguousarray(scifi_batch.offsets - scifi_batch.offsets[0], np.uint32)
+    ut = np.ascontiguousarray(ut_batch.raw[int(ut_batch.offsets[0]):int(ut_batch.offsets[-1])])
+    sf = np.ascontiguousarray(scifi_batch.raw[int(scifi_batch.offsets[0]):int(scifi_batch.offsets[-1])])
+    n_sel = np.zeros(1, np.uint32)
+    lst = np.zeros(max(N, 1), np.uint32)
+    ms = C.c_float()
+    rc = L.ref_gec_run(ut.ctypes.data, ut_off.ctypes.data, sf.ctypes.data, sf_off.ctypes.data, N,
+                       n_sel.ctypes.data, lst.ctypes.data, int(reps), C.byref(ms))
+    if rc != 0:
+        raise RuntimeError(f"ref_gec_run failed: {rc}")
+    return (lst[:int(n_sel[0])], ms.value) if timed else lst[:int(n_sel[0])]
 
 
 def ref_event_clusters(res, e):

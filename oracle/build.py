@@ -55,7 +55,8 @@ def ref_includes():
             "main/include", "stream/gear/include", "stream/setup/include", "cuda/event_model/UT/include",
             "cuda/event_model/SciFi/include", "cuda/UT/PrVeloUT/include", "cuda/UT/common/include",
             "cuda/SciFi/common/include", "cuda/SciFi/PrForward/include", "x86/velo/clustering/include",
-            "cuda/PV/beamlinePV/include", "cuda/PV/common/include", "cuda/utils/float_operations/include"]
+            "cuda/PV/beamlinePV/include", "cuda/PV/common/include", "cuda/utils/float_operations/include",
+            "cuda/global_event_cut/include"]
     return [f"-I{os.path.join(REF, d)}" for d in dirs]
 
 
@@ -80,7 +81,8 @@ def build_ref_x86():
 def build_ref_gpu():
     kernel_dirs = ["cuda/velo/common/src", "cuda/velo/mask_clustering/src", "cuda/velo/calculate_phi_and_sort/src",
                    "cuda/velo/search_by_triplet/src", "cuda/velo/consolidate_tracks/src",
-                   "cuda/velo/simplified_kalman_filter/src", "cuda/utils/prefix_sum/src", "cuda/PV/beamlinePV/src"]
+                   "cuda/velo/simplified_kalman_filter/src", "cuda/utils/prefix_sum/src", "cuda/PV/beamlinePV/src",
+                   "cuda/global_event_cut/src"]
     srcs = []
     for d in kernel_dirs:
         p = os.path.join(REF, d)

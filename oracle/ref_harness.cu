@@ -4,8 +4,8 @@
 // configuration/sequences/Velo.h:5-18 plus velo_kalman_fit_t, with the grid/block shapes,
 // buffer sizes and host synchronisation points of the visitors in
 // stream/visitors/velo/src/*.cu, so the kernels run exactly as the reference runs them.
-// The event list is the identity (init_event_list, InitEventList.cu:7); global_event_cut
-// needs UT/SciFi banks and is not part of the VELO chain.
+// The event list of the VELO chain is the identity (init_event_list, InitEventList.cu:7);
+// global_event_cut runs on its own through ref_gec_run.
 //
 // Every buffer carries a padding tail so that the reference's unchecked writes past an
 // event's region (SURVEY hazards: tracks > 1200, weak tracklets > 500, candidates > 3000)
@@ -23,6 +23,7 @@
 #include "ClusteringCommon.h"
 #include "ConsolidateVelo.cuh"
 #include "EstimateInputSize.cuh"
+#include "GlobalEventCut.cuh"
 #include "FillCandidates.cuh"
 #include "MaskedVeloClustering.cuh"
 #include "PrefixSum.cuh"
@@ -388,4 +389,53 @@ int ref_pv_run(const uint32_t* atomics, const uint32_t* track_hit_number, const 
   cudaStreamDestroy(s);  // the buffers free themselves
   return 0;
 }
+}
+
+// global_event_cut (GlobalEventCut.cu:3-55) launched as GlobalEventCutVisitor.cu does: one
+// block of 32 threads per event, the selected-event counter zeroed first. Offsets are u32, as
+// the reference takes them. The kernel returns from some threads before a __syncthreads when
+// an event's running UT count reaches the cut; callers pass only events whose UT hit total
+// is below the cut, so that every thread of a block reaches every barrier. Outputs: the
+// number of selected events and the event list in the kernel's (atomic) order, and the mean
+// device time of one counter reset + kernel over reps - 1 repetitions after the first.
+extern "C" int ref_gec_run(const void* ut, const uint32_t* ut_offsets, const void* scifi, const uint32_t* scifi_offsets,
+                           uint32_t n_events, uint32_t* n_selected, uint32_t* event_list, int reps, float* ms_per_rep)
+{
+  if (!ut || !ut_offsets || !scifi || !scifi_offsets || !n_selected || !event_list || n_events == 0) return -1;
+  const uint32_t N = n_events;
+  Buf d_ut, d_ut_off, d_sf, d_sf_off, d_n, d_list;
+  CK(d_ut.ensure(ut_offsets[N]));
+  CK(d_ut_off.ensure(4ull * (N + 1)));
+  CK(d_sf.ensure(scifi_offsets[N]));
+  CK(d_sf_off.ensure(4ull * (N + 1)));
+  CK(d_n.ensure(4));
+  CK(d_list.ensure(4ull * N));
+  CK(cudaMemcpy(d_ut.p, ut, ut_offsets[N], cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d_ut_off.p, ut_offsets, 4ull * (N + 1), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d_sf.p, scifi, scifi_offsets[N], cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d_sf_off.p, scifi_offsets, 4ull * (N + 1), cudaMemcpyHostToDevice));
+  cudaEvent_t t0, t1;
+  CK(cudaEventCreate(&t0));
+  CK(cudaEventCreate(&t1));
+  const int R = reps > 0 ? reps : 1;
+  float total_ms = 0.f;
+  for (int rep = 0; rep < R; ++rep) {
+    CK(cudaEventRecord(t0));
+    CK(cudaMemsetAsync(d_n.p, 0, 4));
+    global_event_cut<<<dim3(N), dim3(32)>>>(static_cast<char*>(d_ut.p), static_cast<uint*>(d_ut_off.p),
+                                            static_cast<char*>(d_sf.p), static_cast<uint*>(d_sf_off.p),
+                                            static_cast<uint*>(d_n.p), static_cast<uint*>(d_list.p));
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(t1));
+    CK(cudaEventSynchronize(t1));
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, t0, t1));
+    if (rep > 0 || R == 1) total_ms += t;
+  }
+  if (ms_per_rep) *ms_per_rep = total_ms / (R > 1 ? R - 1 : 1);
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  CK(cudaMemcpy(n_selected, d_n.p, 4, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(event_list, d_list.p, 4ull * N, cudaMemcpyDeviceToHost));
+  return 0;
 }

@@ -1,15 +1,20 @@
 """Generates the committed fixtures under tests/golden/.
 
-  minbias/VP/*.bin, minbias/MC_tracks/*.bin, minbias/mdf/*.mdf
-      the 10 real minbias events shipped with the reference (input/minbias/banks/VP,
-      input/minbias/MC_info/tracks and input/minbias/banks/mdf), copied as data: raw VP
-      banks, their MC truth, and the same events as an MDF file (all banks, compressed).
+  minbias/VP/*.bin, minbias/UT/*.bin, minbias/FTCluster/*.bin, minbias/MC_tracks/*.bin,
+  minbias/mdf/*.mdf
+      the 10 real minbias events shipped with the reference (input/minbias/banks/{VP,UT,
+      FTCluster}, input/minbias/MC_info/tracks and input/minbias/banks/mdf), copied as data:
+      raw banks, their MC truth, and the same events as an MDF file (all banks, compressed).
   ref_gpu_*.npz
       outputs of the reference's own CUDA kernels (oracle/_ref/libvelo_ref_gpu.so) on the
       minbias events and on seeded synthetic events; written by `--ref-gpu` on a GPU box
       (the reference tree is not needed there: the library is prebuilt).
+  ref_gec.npz
+      the events the reference's global_event_cut kernel selects on the minbias events and on
+      GEC_SYNTH_EVENTS seeded synthetic events (gec_synthetic_batches); written by
+      `--ref-gec OUTDIR` on a GPU box.
 
-Usage: python tests/golden/make_golden.py [--minbias] [--ref-gpu OUTDIR]
+Usage: python tests/golden/make_golden.py [--minbias] [--ref-gpu OUTDIR] [--ref-gec OUTDIR]
 """
 import os
 import shutil
@@ -22,7 +27,8 @@ REF = "/root/reference"
 
 
 def copy_minbias():
-    for sub, dst in (("banks/VP", "VP"), ("MC_info/tracks", "MC_tracks"), ("banks/mdf", "mdf")):
+    for sub, dst in (("banks/VP", "VP"), ("banks/UT", "UT"), ("banks/FTCluster", "FTCluster"),
+                     ("MC_info/tracks", "MC_tracks"), ("banks/mdf", "mdf")):
         src = os.path.join(REF, "input/minbias", sub)
         out = os.path.join(HERE, "minbias", dst)
         os.makedirs(out, exist_ok=True)
@@ -76,8 +82,56 @@ def ref_gpu(outdir):
         print(name, b.n_events, "events", res["T"], "tracks")
 
 
+GEC_SYNTH_EVENTS = 2048
+
+
+def gec_synthetic_batches():
+    """(UT, SciFi) batches of the first GEC_SYNTH_EVENTS events of the nu ~ U(2,20) workload
+    (generate_ut_scifi, seed 5) without the events whose UT hit total reaches the cut (the
+    reference kernel is run only on events where every thread reaches every barrier)."""
+    import numpy as np
+    from cuda_hlt_b200 import events
+    from oracle import gec_oracle
+    vp = events.generate_config("pruned_1m", n_events=GEC_SYNTH_EVENTS, with_mc=False)
+    ut, sf = events.generate_ut_scifi(vp, seed=5)
+    counts, _, _ = gec_oracle.run(ut, sf)
+    keep = np.flatnonzero(counts[:, 1] < gec_oracle.MAX_CLUSTERS)
+    return pick(ut, keep), pick(sf, keep), keep
+
+
+def pick(batch, idx):
+    """A batch of the events `idx` of `batch`, in that order."""
+    import numpy as np
+    from cuda_hlt_b200 import events
+    raws = [batch.event(int(i)) for i in idx]
+    off = np.zeros(len(raws) + 1, np.uint64)
+    off[1:] = np.cumsum([r.size for r in raws])
+    return events.EventBatch(np.concatenate(raws) if raws else np.zeros(0, np.uint8), off)
+
+
+def minbias_gec_batches():
+    from cuda_hlt_b200 import events
+    return (events.read_bank_folder(os.path.join(HERE, "minbias", "UT")),
+            events.read_bank_folder(os.path.join(HERE, "minbias", "FTCluster")))
+
+
+def ref_gec(outdir):
+    import numpy as np
+    import oracle
+    ut, sf = minbias_gec_batches()
+    sut, ssf, keep = gec_synthetic_batches()
+    out = dict(minbias_selected=np.sort(oracle.ref_gec_run(ut, sf)),
+               synthetic_events=keep.astype(np.uint32),
+               synthetic_selected=np.sort(oracle.ref_gec_run(sut, ssf)))
+    os.makedirs(outdir, exist_ok=True)
+    np.savez_compressed(os.path.join(outdir, "ref_gec.npz"), **out)
+    print("gec", {k: v.size for k, v in out.items()})
+
+
 if __name__ == "__main__":
     if "--minbias" in sys.argv:
         copy_minbias()
     if "--ref-gpu" in sys.argv:
         ref_gpu(sys.argv[sys.argv.index("--ref-gpu") + 1])
+    if "--ref-gec" in sys.argv:
+        ref_gec(sys.argv[sys.argv.index("--ref-gec") + 1])
