@@ -154,9 +154,10 @@ typedef struct VeloCtx VeloCtx;
 #define VELO_MODE_PLAIN 0  /* exhaustive search_by_triplet (reference semantics) */
 #define VELO_MODE_PRUNED 1 /* learned seed/extension scorer prunes the search */
 
-#define VELO_MAP_AUTO 0    /* autotuned per hit-count bucket */
-#define VELO_MAP_BLOCK 1   /* decode/cluster/sort: one block per event */
-#define VELO_MAP_WARP 2    /* decode/cluster/sort: one warp per event */
+/* Search mapping (velo_set_block_threshold sets the boundary directly). */
+#define VELO_MAP_AUTO 0    /* search: block per event above 1,536 clusters, warp per event below */
+#define VELO_MAP_BLOCK 1   /* search: one block per event */
+#define VELO_MAP_WARP 2    /* search: one warp per event */
 
 typedef struct VeloConfig {
   uint32_t max_events;          /* events per velo_run call */
