@@ -29,7 +29,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_WEIGHTS = os.path.join(HERE, "data", "velo_mlp_weights.bin")
 BATCH = 16384
 THRESHOLDS = (0.1, 0.3, 0.5, 0.7, 0.85)
-MIN_PAIRS = (0, 8, 16, 24, 32)
+MIN_PAIRS = (0, 8, 16, 24, 32, 48, 64, 96)
 
 
 def log(*a):
