@@ -5,7 +5,7 @@ nu ~ U(2,20) workload.
 python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 One step = one pass of the chain over the rank's 1,000,000 synthetic events (seed 4,
-events rank*1000000 ...), in batches of 32,768 events (one CUDA graph per batch). Both
+events rank*1000000 ...), in batches of 65,536 events (one CUDA graph per batch). Both
 forms run on the same device-resident input: the plain chain (reference semantics) and
 the pruned chain (learned seed scorer; events above the scorer's trained occupancy fall
 back to the plain search). Events are independent, so ranks process disjoint event
@@ -42,7 +42,7 @@ METRIC = "VELO events/s on 1 B200, MLP-pruned vs plain at ≤0.2% eff loss; % HB
 UNIT = "events/s"
 WORKLOAD = "pruned_1m"
 N_EVENTS = 1_000_000
-BUCKET = 32768   # events per batch (one CUDA graph); --batch
+BUCKET = 65536   # events per batch (one CUDA graph); --batch
 CHUNK = 4 * BUCKET
 SIDE_BATCH = 16384  # batches of the MC-quality and reference-kernel legs
 E2E_CONTEXTS = 3    # contexts (and streams) in rotation in the end-to-end leg
