@@ -17,7 +17,12 @@ the max over ranks of the elapsed device time. Prints one JSON line (rank 0):
             the head of the workload
   e2e       events/s of the pruned chain through velo_run_host from pinned host memory,
             each batch's consolidated tracks and Kalman states read back to pinned memory
-  roofline, cpu_baseline, clocks, gpu_launches: see DESIGN.md
+  roofline  the stage with the largest serial share (first batches, one stream), its
+            algorithmic bytes per launch over its live CUDA-event time in the timed region,
+            against the measured HBM copy bandwidth; traffic from the committed ncu summary
+  cpu_baseline  the CPU oracle (full chain) on the host cores, and the reference's x86
+            clustering; clocks: nvidia-smi samples during the timed region; gpu_launches:
+            this library's kernel launches in the timed region
 --impl reference times the CPU implementation of the chain (the CPU oracle restating the
 reference kernels; the reference has no CPU tracking) on the host cores, on a bounded
 sample of the same workload.

@@ -8,7 +8,7 @@
 // global_event_cut runs on its own through ref_gec_run.
 //
 // Every buffer carries a padding tail so that the reference's unchecked writes past an
-// event's region (SURVEY hazards: tracks > 1200, weak tracklets > 500, candidates > 3000)
+// event's region (more than 1200 tracks, 500 weak tracklets or 3000 clustering candidates)
 // stay inside this harness's allocations; callers only pass events whose per-module
 // cluster count fits the reference's 500-entry shared phi buffer, which the harness checks
 // on the host before the phi sort runs.

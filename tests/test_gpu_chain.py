@@ -5,7 +5,7 @@ Bit-exact bar (integer work and the float values the reference computes):
     within a module the reference's order for exactly equal phi follows its atomics, so
     only permutations of equal-phi entries are tolerated;
   * tracks: per-event hit-id lists identical after a canonical sort;
-  * beamline (LSQ) and Kalman states: all 12 floats bit for bit (bound of the north star:
+  * beamline (LSQ) and Kalman states: all 12 floats bit for bit (the required bound is
     1e-5 relative), `backward` of the beamline state equal.
 Events the reference leaves undefined (buffer spills, reads outside a module, exact
 scatter ties resolved by atomics) are flagged by both sides and excluded.
