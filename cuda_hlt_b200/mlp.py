@@ -4,7 +4,7 @@ The scorer is a 12 -> 64 -> 64 -> 2 MLP (include/velo_b200.h, VeloMlpWeights). I
 trained on the GPU by the library's own tensor-core kernels (velo_mlp_train / collect /
 gradient / infer) on seeding candidates labelled by the plain search. There is no
 counterpart in the reference; the plain search (search_by_triplet, TrackSeeding.cu:7-200)
-is the fallback and the judge of what pruning costs.
+is the fallback and the yardstick of what pruning costs.
 """
 import ctypes as C
 
