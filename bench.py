@@ -175,7 +175,8 @@ def load_scorer(args):
     if not args.retrain and os.path.exists(path):
         w = mlp.load_weights(path)
         return w, {"weights": os.path.relpath(path, ROOT), "trained": "committed", "seed_threshold": w.seed_threshold,
-                   "min_pairs": w.min_pairs, "max_event_clusters": w.max_event_clusters}
+                   "min_pairs": w.min_pairs, "max_event_clusters": w.max_event_clusters,
+                   "min_event_clusters": w.min_event_clusters}
     log("training the scorer (train_scorer pipeline, 1M samples, 4 epochs)")
     t0 = time.time()
     trainer = mlp.MlpTrainer(1_000_000, seed=1)
@@ -189,8 +190,10 @@ def load_scorer(args):
     w.ext_threshold = 0.0
     val = events.generate_config("mlp_train", n_events=8192, first_event=next_event, threads=threads, with_mc=True)
     (w.seed_threshold, w.min_pairs), _, _ = train_scorer.choose_operating_point(w, val, 0.001)
+    w.min_event_clusters = train_scorer.BENCH_EVENT_GATE
     return w, {"trained": f"in bench: {held} samples, {time.time() - t0:.1f}s", "seed_threshold": w.seed_threshold,
-               "min_pairs": w.min_pairs, "max_event_clusters": max_clusters}
+               "min_pairs": w.min_pairs, "max_event_clusters": max_clusters,
+               "min_event_clusters": w.min_event_clusters}
 
 
 def time_form(vcs, streams, batch_ptrs, args, world, dist, torch, local_rank):

@@ -74,6 +74,7 @@ class VeloMlpWeights(C.Structure):
         ("ext_threshold", C.c_float),
         ("max_event_clusters", C.c_uint32),
         ("min_pairs", C.c_uint32),
+        ("min_event_clusters", C.c_uint32),
     ]
 
 

@@ -700,6 +700,7 @@ int velo_set_mlp(VeloCtx* c, const void* weights_host, size_t bytes)
   c->mlp.ext_logit = w.ext_threshold > 0.f ? logit(w.ext_threshold) : 0.f;
   c->mlp.max_hits = w.max_event_clusters;
   c->mlp.min_pairs = w.min_pairs;
+  c->mlp.min_hits = w.min_event_clusters;
   c->mlp_loaded = true;
   return 0;
 }

@@ -20,7 +20,8 @@
 //                          seed keep, bit 1 extension keep) are kept for the outputs.
 // Events above the scorer's occupancy range append no candidates (the plain search) and get
 // VELO_STATUS_MLP_FALLBACK. Seeds with fewer than min_pairs (h0, h2) combinations are not
-// appended either: they stay seeds, as scoring them would cost more than their pair loop.
+// appended either: they stay seeds, as scoring them would cost more than their pair loop;
+// nor are the seeds of events below min_hits clusters, whose whole search is cheap.
 #pragma once
 #include "velo_mlp.cuh"
 
@@ -89,7 +90,8 @@ __global__ void __launch_bounds__(kFillThreads) fill_candidates_kernel(ChainPoin
           const bool cand = valid && f0 != -1 && f2 != -1;
           if (valid) P.keep[base + h] = cand ? 3u : 2u;  // candidates: verdict from score_candidates
           // seeds whose pair loop is cheaper than their scoring stay kept, unscored
-          const bool append = cand && !fallback && static_cast<uint32_t>((l0 - f0) * (l2 - f2)) >= P.mlp.min_pairs;
+          const bool append = cand && !fallback && nhits >= P.mlp.min_hits &&
+                              static_cast<uint32_t>((l0 - f0) * (l2 - f2)) >= P.mlp.min_pairs;
           // one atomic per warp for the rows of its candidates; the features follow in
           // candidate_features, densely
           const uint32_t bal = __ballot_sync(0xFFFFFFFFu, append);

@@ -54,6 +54,7 @@ struct MlpDevice {
   uint32_t use_ext;        // extension pruning on
   uint32_t max_hits;       // events with more clusters fall back to the plain search
   uint32_t min_pairs;      // seeds with fewer (h0, h2) pairs are kept unscored
+  uint32_t min_hits;       // events with fewer clusters are not scored (every seed kept)
 };
 
 // Clusters after the phi sort: position and phi of a cluster in one 16-byte record (one

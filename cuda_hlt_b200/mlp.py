@@ -31,7 +31,7 @@ def weights_to_dict(w):
                 w1=np.ctypeslib.as_array(w.w1).copy(), w2=np.ctypeslib.as_array(w.w2).copy(),
                 w3=np.ctypeslib.as_array(w.w3).copy(), seed_threshold=float(w.seed_threshold),
                 ext_threshold=float(w.ext_threshold), max_event_clusters=int(w.max_event_clusters),
-                min_pairs=int(w.min_pairs))
+                min_pairs=int(w.min_pairs), min_event_clusters=int(w.min_event_clusters))
 
 
 def dict_to_weights(d):
@@ -42,6 +42,7 @@ def dict_to_weights(d):
     w.ext_threshold = d.get("ext_threshold", 0.0)
     w.max_event_clusters = d.get("max_event_clusters", 0xFFFFFFFF)
     w.min_pairs = d.get("min_pairs", 0)
+    w.min_event_clusters = d.get("min_event_clusters", 0)
     return w
 
 
@@ -53,8 +54,11 @@ def save_weights(w, path):
 def load_weights(path):
     with open(path, "rb") as f:
         blob = f.read()
-    if len(blob) != C.sizeof(_lib.VeloMlpWeights):
-        raise MlpError(f"{path}: {len(blob)} bytes, expected {C.sizeof(_lib.VeloMlpWeights)}")
+    size = C.sizeof(_lib.VeloMlpWeights)
+    if len(blob) == size - 4:  # files written before min_event_clusters: every event scored
+        blob += bytes(4)
+    if len(blob) != size:
+        raise MlpError(f"{path}: {len(blob)} bytes, expected {size}")
     return _lib.VeloMlpWeights.from_buffer_copy(blob)
 
 

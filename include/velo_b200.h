@@ -290,6 +290,8 @@ typedef struct VeloMlpWeights {
   float ext_threshold;          /* probability; 0 disables extension pruning */
   uint32_t max_event_clusters;  /* occupancy limit of the trained range */
   uint32_t min_pairs;           /* score only seeds with |h0 window| x |h2 window| >= this */
+  uint32_t min_event_clusters;  /* score only in events with at least this many clusters (0: all);
+                                   smaller events keep every seed, as in the plain search */
 } VeloMlpWeights;
 
 /* Loads the scorer (weights_host -> VeloMlpWeights, bytes == sizeof(VeloMlpWeights));

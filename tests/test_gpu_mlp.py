@@ -214,6 +214,23 @@ def test_scoring_gate():
         n_small += int(small.sum())
         n_large += int((~small).sum())
     assert n_small > 0 and n_large > 0
+    # event gate: events below min_event_clusters keep every seed (the plain result), the
+    # others lose every seed to the scorer (no tracks)
+    n_hits = res["module_num"].reshape(-1, 52).sum(axis=1)
+    cut = int(np.median(n_hits))
+    d["min_pairs"] = 0
+    d["min_event_clusters"] = cut
+    ev = run_mode(b, chain.MODE_PRUNED, mlp.dict_to_weights(d))
+    plain = run_mode(b, chain.MODE_PLAIN)
+    below = above = 0
+    for e in range(b.n_events):
+        if n_hits[e] < cut:
+            assert sorted(chain.event_tracks(ev, e)) == sorted(chain.event_tracks(plain, e)), e
+            below += 1
+        else:
+            assert len(chain.event_tracks(ev, e)) == 0, e
+            above += 1
+    assert below > 0 and above > 0
 
 
 def test_trained_scorer_prunes_at_no_efficiency_cost():
