@@ -1,6 +1,7 @@
 """CPU checks of the scorer's oracle (oracle/mlp_oracle.py): bf16 rounding, the float64
 gradient against central finite differences, and the bf16 restatement against float64."""
 import numpy as np
+import pytest
 
 from oracle import mlp_oracle
 
@@ -76,3 +77,21 @@ def test_features_of_a_straight_track():
     fr = feats[on_line[0]]
     assert abs(fr[0] - tx) < 1e-5 and abs(fr[1] - ty) < 1e-5
     assert fr[2] < 1e-3 and fr[5] == 2 and fr[9] == 2 and fr[10] == 2 and fr[11] == 2
+
+
+def test_committed_weights_file_and_old_format(tmp_path):
+    """The committed scorer file holds the operating point; a file written before the event
+    gate existed (4 bytes shorter) loads with the gate at 0 (every event scored)."""
+    from cuda_hlt_b200 import mlp, train_scorer
+    w = mlp.load_weights(train_scorer.DEFAULT_WEIGHTS)
+    assert 0.0 < w.seed_threshold < 1.0
+    assert w.min_event_clusters == train_scorer.BENCH_EVENT_GATE
+    assert w.max_event_clusters > w.min_event_clusters
+    old = tmp_path / "old.bin"
+    old.write_bytes(bytes(w)[:-4])
+    w_old = mlp.load_weights(str(old))
+    assert w_old.min_event_clusters == 0 and w_old.min_pairs == w.min_pairs
+    bad = tmp_path / "bad.bin"
+    bad.write_bytes(bytes(w)[:-8])
+    with pytest.raises(mlp.MlpError):
+        mlp.load_weights(str(bad))
