@@ -149,6 +149,7 @@ GPU_SYMBOLS = [
     "velo_set_block_threshold",
     "velo_set_decode_warps",
     "velo_last_launch_count",
+    "velo_check_wait_timeout",
     "velo_search_static",
     "velo_version",
     "velo_set_mode",
@@ -248,6 +249,8 @@ def gpu_lib():
         lib.velo_set_decode_warps.restype = C.c_int
         lib.velo_last_launch_count.argtypes = [P, C.POINTER(C.c_uint32)]
         lib.velo_last_launch_count.restype = C.c_int
+        lib.velo_check_wait_timeout.argtypes = [P, C.c_uint32, P]
+        lib.velo_check_wait_timeout.restype = C.c_int
         lib.velo_search_static.argtypes = [P] * 4 + [C.c_uint32] + [P] * 5
         lib.velo_search_static.restype = C.c_int
         lib.velo_version.argtypes = []

@@ -315,6 +315,19 @@ void size_decode_grid(VeloCtx* c)
   c->decode_blocks = static_cast<uint32_t>(std::max(1, occ) * c->sm_count);
 }
 
+// A bounded wait that runs out: an mbarrier that nothing arrives on, waited for with
+// mbar_wait_parity (the wait of the scorer's copies and tensor-core steps) for `polls` polls;
+// the kernel then sets the error bit the scorer sets on a timeout and returns. Nothing is in
+// flight when it gives up, so it exits cleanly.
+__global__ void wait_timeout_kernel(uint32_t* error, uint32_t polls)
+{
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) mbar_init1(&bar);
+  __syncthreads();
+  const bool done = mbar_wait_parity(&bar, 0, polls);
+  if (!done && threadIdx.x == 0) atomicOr(error, kErrorMlpTimeout);
+}
+
 void drop_graphs(VeloCtx* c)
 {
   cudaSetDevice(c->device);
@@ -792,6 +805,18 @@ int velo_set_block_threshold(VeloCtx* c, uint32_t clusters)
   if (!c) return VELO_ERR_INVALID;
   if (clusters != c->block_threshold) drop_graphs(c);  // the launch sequence changes
   c->block_threshold = clusters;
+  return 0;
+}
+
+int velo_check_wait_timeout(VeloCtx* c, uint32_t polls, void* stream)
+{
+  if (!c || polls == 0 || polls > (1u << 20)) return VELO_ERR_INVALID;
+  if (cudaSetDevice(c->device) != cudaSuccess) return VELO_ERR_CUDA;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  c->last_stream = s;
+  VCK(cudaMemsetAsync(c->d_queue + 6, 0, sizeof(uint32_t), s));
+  wait_timeout_kernel<<<1, 32, 0, s>>>(c->d_queue + 6, polls);
+  VCK(cudaGetLastError());
   return 0;
 }
 

@@ -547,7 +547,16 @@ extern "C" int velo_check_tracks(const void* mc_blob, const uint64_t* mc_offsets
       for (uint32_t h : hits) id_map.emplace_back(h, static_cast<uint32_t>(mcps.size()));
       mcps.push_back(m);
     }
-    std::sort(id_map.begin(), id_map.end());
+    // The association map is built and sorted as the reference's MCAssociator builds it
+    // (checker/tracking/src/MCAssociator.cpp:13-29): entries appended particle by particle in
+    // file order, sorted on the id alone with std::sort, looked up with lower_bound. An id
+    // that several particles share (real data has some) counts for the particle whose entry
+    // that sort leaves first; comparing the index too would pick another particle for some
+    // of them and change the weight of those tracks.
+    std::sort(id_map.begin(), id_map.end(),
+              [](const std::pair<uint32_t, uint32_t>& a, const std::pair<uint32_t, uint32_t>& b) {
+                return a.first < b.first;
+              });
     auto is_electron = [](const ParsedMcp& m) { return std::abs(m.pid) == 11; };
     auto cat_long = [&](const ParsedMcp& m) { return m.is_long && !is_electron(m) && m.eta > 2.f && m.eta < 5.f; };
     auto cat_velo = [&](const ParsedMcp& m) { return m.has_velo && !is_electron(m); };
@@ -562,7 +571,8 @@ extern "C" int velo_check_tracks(const void* mc_blob, const uint64_t* mc_offsets
       std::map<uint32_t, uint32_t> counts;
       uint32_t matched = 0;
       for (uint32_t h = track_hit_offsets[t]; h < track_hit_offsets[t + 1]; ++h) {
-        auto it = std::lower_bound(id_map.begin(), id_map.end(), std::make_pair(hit_ids[h], 0u));
+        auto it = std::lower_bound(id_map.begin(), id_map.end(), hit_ids[h],
+                                   [](const std::pair<uint32_t, uint32_t>& a, uint32_t id) { return a.first < id; });
         if (it == id_map.end() || it->first != hit_ids[h]) continue;
         ++matched;
         ++counts[it->second];

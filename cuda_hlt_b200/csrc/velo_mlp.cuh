@@ -75,11 +75,11 @@ __device__ __forceinline__ void mbar_init1(uint64_t* mbar)
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
-// Waits for the phase `parity` of the barrier to complete; false after kMbarSpinLimit polls.
-__device__ __forceinline__ bool mbar_wait_parity(uint64_t* mbar, uint32_t parity)
+// Waits for the phase `parity` of the barrier to complete; false after `limit` polls.
+__device__ __forceinline__ bool mbar_wait_parity(uint64_t* mbar, uint32_t parity, uint32_t limit = kMbarSpinLimit)
 {
   const uint32_t a = smem_u32(mbar);
-  for (uint32_t i = 0; i < kMbarSpinLimit; ++i) {
+  for (uint32_t i = 0; i < limit; ++i) {
     uint32_t done;
     asm volatile(
       "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"

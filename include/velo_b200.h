@@ -356,6 +356,13 @@ int velo_set_block_threshold(VeloCtx* ctx, uint32_t clusters);
  * (cuda_hlt_b200/autotune.py) from decode timings on a sample batch. */
 int velo_set_decode_warps(VeloCtx* ctx, uint32_t warps);
 
+/* Diagnostics of the error path of the bounded device waits: runs one kernel that waits, for
+ * `polls` polls (1 .. 2^20), on a barrier that nothing completes, with the wait function of
+ * the scorer kernels; the wait runs out, the kernel records the timeout and returns, and the
+ * next velo_sync returns VELO_ERR_DEVICE_TIMEOUT. The context stays usable: the next run
+ * clears the error. No counterpart in the reference (its kernels report nothing). */
+int velo_check_wait_timeout(VeloCtx* ctx, uint32_t polls, void* stream);
+
 /* Kernel launch count of the last run (all kernels of this library). */
 int velo_last_launch_count(VeloCtx* ctx, uint32_t* n);
 

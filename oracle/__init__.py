@@ -17,6 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_LIB = os.path.join(HERE, "liboracle.so")
 REF_GPU_LIB = os.path.join(HERE, "_ref", "libvelo_ref_gpu.so")
 REF_X86_LIB = os.path.join(HERE, "_ref", "libvelo_ref_x86.so")
+REF_CHECKER_LIB = os.path.join(HERE, "_ref", "libvelo_ref_checker.so")
 
 NM = 52
 F_BAD_RAW = 1 << 0
@@ -309,3 +310,38 @@ def ref_x86_sp_patterns():
     fy = np.zeros(512, np.float32)
     L.ref_x86_sp_patterns(pat.ctypes.data, siz.ctypes.data, fx.ctypes.data, fy.ctypes.data)
     return pat, siz, fx, fy
+
+
+_ref_checker = None
+
+
+def ref_check_velo_tracks(batch, event_track_offsets, track_hit_offsets, hit_ids, max_categories=64):
+    """The reference's own TrackCheckerVelo (oracle/_ref/libvelo_ref_checker.so, built from
+    checker/tracking without ROOT) on consolidated tracks against the batch's MC_info blobs.
+    Returns dict(categories={name: (reconstructible, found, clones)}, tracks, ghosts,
+    ghost_per_event)."""
+    global _ref_checker
+    if _ref_checker is None:
+        if not os.path.exists(REF_CHECKER_LIB):
+            raise RuntimeError(f"{REF_CHECKER_LIB} missing: run oracle/build.py where the reference tree exists")
+        L = C.CDLL(REF_CHECKER_LIB)
+        P = C.c_void_p
+        L.ref_check_velo_tracks.argtypes = [P, P, C.c_uint32, P, P, P, C.c_uint32, P, P, P, C.POINTER(C.c_float)]
+        L.ref_check_velo_tracks.restype = C.c_int
+        _ref_checker = L
+    evt = np.ascontiguousarray(event_track_offsets, np.uint32)
+    tho = np.ascontiguousarray(track_hit_offsets, np.uint32)
+    ids = np.ascontiguousarray(hit_ids, np.uint32)
+    mco = np.ascontiguousarray(batch.mc_offsets, np.uint64)
+    names = np.zeros(64 * max_categories, np.uint8)
+    counts = np.zeros(3 * max_categories, np.uint64)
+    totals = np.zeros(2, np.uint64)
+    gpe = C.c_float()
+    n = _ref_checker.ref_check_velo_tracks(batch.mc.ctypes.data, mco.ctypes.data, batch.n_events, evt.ctypes.data,
+                                           tho.ctypes.data, ids.ctypes.data, max_categories, names.ctypes.data,
+                                           counts.ctypes.data, totals.ctypes.data, C.byref(gpe))
+    cats = {}
+    for i in range(min(n, max_categories)):
+        name = bytes(names[64 * i:64 * (i + 1)]).split(b"\0")[0].decode()
+        cats[name] = tuple(int(v) for v in counts[3 * i:3 * i + 3])
+    return dict(categories=cats, tracks=int(totals[0]), ghosts=int(totals[1]), ghost_per_event=gpe.value)

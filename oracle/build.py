@@ -2,6 +2,8 @@
 
   oracle/liboracle.so            CPU restatement of the reference chain (velo_oracle.cpp); always built.
   oracle/_ref/libvelo_ref_x86.so the reference's x86 clustering, compiled from the reference tree.
+  oracle/_ref/libvelo_ref_checker.so the reference's VELO track checker (checker/tracking, host
+                                 code, no ROOT) with ref_checker.cpp.
   oracle/_ref/libvelo_ref_gpu.so the reference's VELO CUDA kernels, compiled from the reference tree
                                  for sm_100a with the reference's own CUDA flags (CMakeLists.txt:119:
                                  --use_fast_math --expt-relaxed-constexpr --maxrregcount=63, -O3 -DNDEBUG,
@@ -17,7 +19,10 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("VELO_REFERENCE_TREE", "/root/reference")
+# The reference tree: VELO_REFERENCE_TREE, else a checkout named "reference" beside this
+# repository. Where neither exists (the GPU box) the prebuilt _ref libraries are used as they are.
+REF = os.environ.get("VELO_REFERENCE_TREE",
+                     os.path.normpath(os.path.join(HERE, os.pardir, os.pardir, "reference")))
 OUT = os.path.join(HERE, "_ref")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 REF_CUDA_FLAGS = ["-rdc=true", "--use_fast_math", "--expt-relaxed-constexpr", "--maxrregcount=63", "-O3", "-DNDEBUG",
@@ -78,6 +83,21 @@ def build_ref_x86():
     return lib
 
 
+def build_ref_checker():
+    """The reference's VELO track checker (checker/tracking: TrackChecker, its categories, the
+    MC associator and the MC_info reader, with main/src/Logger.cpp), host code built without
+    ROOT, with ref_checker.cpp to call it."""
+    srcs = [os.path.join(REF, "checker/tracking/src", f) for f in
+            ("TrackChecker.cpp", "CategoriesTrackChecker.cpp", "MCAssociator.cpp", "MCEvent.cpp")]
+    srcs.append(os.path.join(REF, "main/src/Logger.cpp"))
+    wrapper = os.path.join(HERE, "ref_checker.cpp")
+    lib = os.path.join(OUT, "libvelo_ref_checker.so")
+    if newer(lib, srcs + [wrapper]):
+        sh(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", f"-I{os.path.join(REF, 'checker/tracking/include')}",
+            f"-I{os.path.join(REF, 'main/include')}", "-I/usr/local/cuda/include"] + srcs + [wrapper, "-o", lib])
+    return lib
+
+
 def build_ref_gpu():
     kernel_dirs = ["cuda/velo/common/src", "cuda/velo/mask_clustering/src", "cuda/velo/calculate_phi_and_sort/src",
                    "cuda/velo/search_by_triplet/src", "cuda/velo/consolidate_tracks/src",
@@ -127,6 +147,7 @@ def build(ref=True):
     if ref and os.path.isdir(REF):
         os.makedirs(OUT, exist_ok=True)
         built.append(build_ref_x86())
+        built.append(build_ref_checker())
         built.append(build_ref_gpu())
     return built
 

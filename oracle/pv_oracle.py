@@ -20,6 +20,20 @@ MAX_TRACK_Z0_ERR, MIN_DENSITY, MIN_DIP_DENSITY, MIN_TRACKS_IN_SEED = F(1.5), F(1
 MAX_VERTEX_RHO2, MAX_FIT_ITER, MAX_DELTA_CHI2, MIN_WEIGHT = F(0.09), 2, F(9.0), F(0.3)
 ORDER, MIN_TRACKS_PER_VERTEX, MAX_VERTICES = 2, 5, 32
 
+# Singular cases met since reset_singular(), by kind. The fp32 Kalman covariances of a few
+# tracks are negative or zero (the simplified Kalman fit is ill-conditioned), so:
+#   zweight    a track's z weight is not positive: the reference's 1/sqrt gives NaN or inf and
+#              its "zerr < max" test drops the track; dropped here by an explicit test;
+#   weight     a fit weight is not finite (exp overflows on a negative weight matrix): the
+#              reference carries the NaN or inf into the vertex sums, and so does this code,
+#              with the overflow counted instead of warned about.
+SINGULAR = dict(zweight=0, weight=0)
+
+
+def reset_singular():
+    for k in SINGULAR:
+        SINGULAR[k] = 0
+
 
 def extrapolate(k):
     """k: dict of float32 arrays x, y, tx, ty, c00, c20, c22, c11, c31, c33, z of the event's
@@ -49,6 +63,9 @@ def histogram(t):
             continue
         zbin = (z - ZMIN) / DZ
         zweight = F(t["tx"][i]) * F(t["tx"][i]) * F(t["w00"][i]) + F(t["ty"][i]) * F(t["ty"][i]) * F(t["w11"][i])
+        if not zweight > F(0):  # 1/sqrt is NaN or inf: the reference's test below fails too
+            SINGULAR["zweight"] += 1
+            continue
         zerr = F(1) / np.sqrt(F(zweight))
         if not zerr < MAX_TRACK_Z0_ERR:
             continue
@@ -158,8 +175,11 @@ def fit(t, seeds):
                 odz = seeds - F(t["z"][i])
                 ox = F(0) - (F(t["x"][i]) + tx * odz)
                 oy = F(0) - (F(t["y"][i]) + ty * odz)
-                denom = np.exp(-cut * F(0.5)) + np.sum(np.exp(-(ox * ox * w00 + oy * oy * w11) * F(0.5)), dtype=F)
-                w = np.exp(-chi2 * F(0.5)) / denom
+                with np.errstate(over="ignore", invalid="ignore"):
+                    denom = np.exp(-cut * F(0.5)) + np.sum(np.exp(-(ox * ox * w00 + oy * oy * w11) * F(0.5)), dtype=F)
+                    w = np.exp(-chi2 * F(0.5)) / denom
+                if not (np.isfinite(denom) and np.isfinite(w)):
+                    SINGULAR["weight"] += 1
                 if w < MIN_WEIGHT:
                     continue
                 g += np.array([rx * w00, ry * w11, -tx * rx * w00 - ty * ry * w11], F) * w

@@ -37,6 +37,8 @@ def golden_batch(name):
         return events.generate_config("plain_1k", n_events=64)
     if name == "batched":
         return events.generate_config("batched_500k", n_events=32)
+    if name == "pruned1m":
+        return events.generate_config("pruned_1m", n_events=64)
     raise KeyError(name)
 
 

@@ -14,7 +14,7 @@
       GEC_SYNTH_EVENTS seeded synthetic events (gec_synthetic_batches); written by
       `--ref-gec OUTDIR` on a GPU box.
 
-Usage: python tests/golden/make_golden.py [--minbias] [--ref-gpu OUTDIR] [--ref-gec OUTDIR]
+Usage: python tests/golden/make_golden.py [--minbias] [--ref-gpu OUTDIR [--only NAME,...]] [--ref-gec OUTDIR]
 """
 import os
 import shutil
@@ -23,7 +23,9 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
-REF = "/root/reference"
+# the reference tree (read only by --minbias): VELO_REFERENCE_TREE, else a checkout named
+# "reference" beside this repository
+REF = os.environ.get("VELO_REFERENCE_TREE", os.path.normpath(os.path.join(ROOT, os.pardir, "reference")))
 
 
 def copy_minbias():
@@ -38,10 +40,12 @@ def copy_minbias():
 
 def synthetic_batches():
     from cuda_hlt_b200 import events
-    # 64 events of the 1,000-event nu=7.6 workload (seed 0) and 32 events of the
-    # nu ~ U(2,15) workload, first events of each stream.
+    # 64 events of the 1,000-event nu=7.6 workload (seed 0), 32 events of the
+    # nu ~ U(2,15) workload and 64 of the nu ~ U(2,20) workload (seed 4, about a quarter of
+    # them above nu = 15), first events of each stream.
     return {"plain": events.generate_config("plain_1k", n_events=64),
-            "batched": events.generate_config("batched_500k", n_events=32)}
+            "batched": events.generate_config("batched_500k", n_events=32),
+            "pruned1m": events.generate_config("pruned_1m", n_events=64)}
 
 
 def compact_reference(res, n_events):
@@ -68,13 +72,15 @@ def compact_reference(res, n_events):
     return out
 
 
-def ref_gpu(outdir):
+def ref_gpu(outdir, only=None):
     import numpy as np
     import oracle
     from cuda_hlt_b200 import events
     geo = events.load_geometry()
     batches = {"minbias": events.read_bank_folder(os.path.join(HERE, "minbias", "VP"))}
     batches.update(synthetic_batches())
+    if only:
+        batches = {k: v for k, v in batches.items() if k in only}
     os.makedirs(outdir, exist_ok=True)
     for name, b in batches.items():
         res, _ = oracle.ref_gpu_run(b, geo)
@@ -132,6 +138,7 @@ if __name__ == "__main__":
     if "--minbias" in sys.argv:
         copy_minbias()
     if "--ref-gpu" in sys.argv:
-        ref_gpu(sys.argv[sys.argv.index("--ref-gpu") + 1])
+        only = sys.argv[sys.argv.index("--only") + 1].split(",") if "--only" in sys.argv else None
+        ref_gpu(sys.argv[sys.argv.index("--ref-gpu") + 1], only)
     if "--ref-gec" in sys.argv:
         ref_gec(sys.argv[sys.argv.index("--ref-gec") + 1])
