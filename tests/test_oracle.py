@@ -21,7 +21,7 @@ needs_ref_x86 = pytest.mark.skipif(not os.path.exists(oracle.REF_X86_LIB), reaso
 
 
 @needs_ref_x86
-@pytest.mark.parametrize("which", ["minbias", "plain", "batched"])
+@pytest.mark.parametrize("which", ["minbias", "plain", "batched", "pruned1m"])
 def test_oracle_clusters_equal_reference_x86(geometry, which):
     b = golden_batch(which)
     r = oracle.run(b, geometry, stages=1)
@@ -42,7 +42,7 @@ def _oracle_modules(r, e):
     return out
 
 
-@pytest.mark.parametrize("which", ["minbias", "plain", "batched"])
+@pytest.mark.parametrize("which", ["minbias", "plain", "batched", "pruned1m"])
 def test_oracle_vs_reference_gpu_golden(geometry, which):
     g = load_golden(which)
     b = golden_batch(which)
@@ -74,7 +74,7 @@ ORACLE_STATE_Q99 = {
 }
 
 
-@pytest.mark.parametrize("which", ["minbias", "plain"])
+@pytest.mark.parametrize("which", ["minbias", "plain", "pruned1m"])
 def test_oracle_states_vs_reference_gpu_golden(geometry, which):
     g = load_golden(which)
     b = golden_batch(which)
