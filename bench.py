@@ -233,10 +233,16 @@ def time_form(vcs, streams, batch_ptrs, args, world, dist, torch, local_rank):
     elapsed_ms = start.elapsed_time(end)
     if world > 1:
         elapsed_ms = shard.max_over_ranks(elapsed_ms, dist, torch.device("cuda", local_rank))
+    # every timed launch records its stage events (the contexts keep the last 64): per-launch
+    # means of each context times its launches per step give the stage times of one step
     stages = {}
-    for vc in vcs:
-        for k, v in vc.stage_times().items():
-            stages[k] = stages.get(k, 0) + v
+    for j, vc in enumerate(vcs):
+        st = vc.stage_times()
+        runs = max(1, st.pop("runs"))
+        per_step = sum(1 for k in range(len(batch_ptrs)) if k % len(vcs) == j)
+        for k, v in st.items():
+            stages[k] = stages.get(k, 0) + v / runs * per_step
+    stages["runs"] = len(batch_ptrs)  # launches per step
     return elapsed_ms, stages, clocks.summary()
 
 
@@ -260,16 +266,11 @@ def roofline(stages, census, n_events, n_batches, peak, peak_kind, traffic_table
     """HBM roofline of the dominant kernel of one form (per launch = one batch): the stage
     with the largest serial share (`shares`), timed live over the timed region."""
     clusters, tracks, track_hits, raw_bytes = (census[k] for k in ("clusters", "tracks", "track_hits", "raw_bytes"))
-    per = {  # algorithmic bytes of one step, per stage
-        "decode_cluster_sort": raw_bytes + 16 * clusters,
-        "fill_candidates": 16 * clusters + 8 * clusters,
-        "search_by_triplet": 16 * clusters + 8 * clusters + 2 * track_hits + 2 * tracks,
-        "event_scan": 16 * n_events,
-        "consolidate_fit": 34 * track_hits + 98 * tracks + 8 * tracks,
-        "pv_beamline": 49 * tracks,  # the Kalman states read once (the stage is off in both timed forms)
-    }
+    per = stage_bytes(census, n_events)  # algorithmic bytes of one step, per stage
+    per["pv_beamline"] = 49 * tracks  # the Kalman states read once (the stage is off in both timed forms)
     stage_ms = {k: stages[k] for k in chain.STAGES}
-    dominant = max(shares, key=shares.get) if shares else max(stage_ms, key=stage_ms.get)
+    ranked = shares if shares else stage_ms
+    dominant = max((k for k in ranked if k in per), key=ranked.get)
     avg_launch_ms = stage_ms[dominant] / max(1, stages["runs"])
     alg_bytes_launch = per[dominant] / n_batches
     achieved = alg_bytes_launch / (avg_launch_ms / 1e3) / 1e9
@@ -284,24 +285,44 @@ def roofline(stages, census, n_events, n_batches, peak, peak_kind, traffic_table
                                           + 8 * n_batches) / n_events}, stage_ms
 
 
+# Label-pruned forms (VELO_MODE_LABELS: the plain search's own labels of the batch, a perfect
+# scorer at no cost): (name, prune extensions too, events above the scorer's trained
+# occupancy fall back to the plain search as in the pruned form)
+LABEL_FORMS = (("labels_seed", False, True), ("labels_seed_ext", True, True),
+               ("labels_seed_ext_all_events", True, False))
+
+
 def run_quality(weights, n, threads):
-    """Long-track efficiency and ghost rate of both forms against generator truth on the
-    first n events of the workload (with MC truth)."""
+    """Long-track efficiency and ghost rate of both forms, and of the label-pruned forms,
+    against generator truth on the first n events of the workload (with MC truth)."""
     rows = {"plain": [], "pruned": []}
+    rows.update({name: [] for name, _, _ in LABEL_FORMS})
+
+    def add(name, b, res):
+        c = chain.check_tracks(b, res)
+        rows[name].append((c.long_reconstructible, c.long_found, c.tracks, c.ghosts, c.velo_reconstructible,
+                           c.velo_found))
+
     for a in range(0, n, SIDE_BATCH):
         m = min(SIDE_BATCH, n - a)
         b = events.generate_config(WORKLOAD, n_events=m, first_event=a, threads=threads, with_mc=True)
+        vc = chain.VeloChain(max_events=m, max_raw_bytes=int(b.raw.size) + 4096)
+        vc.set_mlp(weights)
         for name, mode in (("plain", chain.MODE_PLAIN), ("pruned", chain.MODE_PRUNED)):
-            vc = chain.VeloChain(max_events=m, max_raw_bytes=int(b.raw.size) + 4096)
-            vc.set_mlp(weights)
             vc.set_mode(mode)
             vc.run_host(b)
             vc.sync()
-            res = vc.results(clusters=False)
-            vc.close()
-            c = chain.check_tracks(b, res)
-            rows[name].append((c.long_reconstructible, c.long_found, c.tracks, c.ghosts, c.velo_reconstructible,
-                               c.velo_found))
+            add(name, b, vc.results(clusters=False))
+        for name, ext, fallback in LABEL_FORMS:
+            vc.set_mode(chain.MODE_PLAIN)
+            vc.run_host(b)
+            vc.sync()
+            vc.capture_labels(ext=ext, max_event_clusters=weights.max_event_clusters if fallback else 0xFFFFFFFF)
+            vc.set_mode(chain.MODE_LABELS)
+            vc.run_host(b)
+            vc.sync()
+            add(name, b, vc.results(clusters=False))
+        vc.close()
     out = {}
     for name, r in rows.items():
         lr, lf, t, g, vr, vf = (sum(x[i] for x in r) for i in range(6))
@@ -311,6 +332,61 @@ def run_quality(weights, n, threads):
     out["long_efficiency_loss"] = out["plain"]["long_efficiency"] - out["pruned"]["long_efficiency"]
     out["ghost_rate_change"] = out["pruned"]["ghost_rate"] - out["plain"]["ghost_rate"]
     return out
+
+
+def pruning_ceiling(weights, batch_ptrs, max_batch_bytes, threshold, decode_warps, stream, torch, n_batches=2):
+    """Device time per stage of the plain chain, the scorer-pruned chain and the label-pruned
+    chains (the plain search's own labels: what a perfect scorer at no cost would save), on
+    the first batches of the workload, one after another on one stream (CUDA events per
+    stage, mean of 3 runs per batch after one untimed run)."""
+    vc = chain.VeloChain(max_events=BUCKET, max_raw_bytes=max_batch_bytes + 4096)
+    vc.set_mlp(weights)
+    vc.set_block_threshold(threshold)
+    vc.set_decode_warps(decode_warps)
+    forms = ["plain", "pruned"] + [name for name, _, _ in LABEL_FORMS]
+    acc = {f: {} for f in forms}
+    n_events = 0
+
+    def timed(name, raw_p, off_p, n):
+        vc.run_device(raw_p, off_p, n, stream)
+        torch.cuda.synchronize()
+        vc.set_timing(True)
+        for _ in range(3):
+            vc.run_device(raw_p, off_p, n, stream)
+        vc.sync(clusters=False)
+        st = vc.stage_times()
+        runs = max(1, st.pop("runs"))
+        for k, v in st.items():
+            acc[name][k] = acc[name].get(k, 0.0) + v / runs
+        vc.set_timing(False)
+
+    for raw_p, off_p, n in batch_ptrs[:n_batches]:
+        n_events += n
+        for name, mode in (("plain", chain.MODE_PLAIN), ("pruned", chain.MODE_PRUNED)):
+            vc.set_mode(mode)
+            timed(name, raw_p, off_p, n)
+        for name, ext, fallback in LABEL_FORMS:
+            vc.set_mode(chain.MODE_PLAIN)
+            vc.run_device(raw_p, off_p, n, stream)
+            vc.sync(clusters=False)
+            vc.capture_labels(ext=ext, max_event_clusters=weights.max_event_clusters if fallback else 0xFFFFFFFF)
+            vc.set_mode(chain.MODE_LABELS)
+            timed(name, raw_p, off_p, n)
+    vc.close()
+    stage_keys = ("decode_cluster_sort", "fill_candidates", "search_by_triplet", "event_scan", "consolidate_fit")
+    stages = {f: {k: acc[f].get(k, 0.0) for k in stage_keys} for f in forms}
+    chain_ms = {f: sum(stages[f].values()) for f in forms}
+    return {"events": n_events, "batches": n_batches,
+            "timing": "one stream, stages bracketed by CUDA events, mean of 3 runs per batch, summed over batches",
+            "forms": {"plain": "reference semantics", "pruned": "committed scorer",
+                      "labels_seed": "seeds kept only where the plain search found a track (perfect seed scorer); "
+                                     "events above the trained occupancy run the plain search",
+                      "labels_seed_ext": "and extension candidates only where the plain search extended a track",
+                      "labels_seed_ext_all_events": "both, on every event (no occupancy fallback)"},
+            "stages_ms": stages, "chain_ms": chain_ms,
+            "speedup_vs_plain": {f: chain_ms["plain"] / chain_ms[f] for f in forms},
+            "search_speedup_vs_plain": {f: stages["plain"]["search_by_triplet"] / stages[f]["search_by_triplet"]
+                                        for f in forms}}
 
 
 def run_ours(args, rank, world, local_rank):
@@ -380,9 +456,10 @@ def run_ours(args, rank, world, local_rank):
         roof, stage_ms = roofline(stages, census, n_events, n_batches, peak, peak_kind, traffic_table, shares)
         forms[name] = {"value": n_events * world * args.steps / (elapsed_ms / 1e3),
                        "ms_per_step": elapsed_ms / args.steps,
-                       # one graph per batch holds the stage events of its last launch: the sum over
-                       # the graphs is one step (stages of the two streams overlap in time)
+                       # per-launch means times launches per step (stages of the two streams
+                       # overlap in time)
                        "stages_ms_per_step": stage_ms,
+                       "graphs": sum(v.graph_count() for v in vcs),
                        "roofline": roof, "census_per_step": census,
                        "search_mapping": {"block_above_clusters": threshold,
                                           "search_ms_per_threshold": {str(k): v for k, v in tune_ms.items()}},
@@ -397,6 +474,12 @@ def run_ours(args, rank, world, local_rank):
     # ---- track quality of both forms on the MC-carrying head of the workload ----
     quality = run_quality(weights, args.quality_events, threads) if rank == 0 and args.quality_events > 0 else None
 
+    # ---- per-stage times of every form, and the ceiling of pruning (label-pruned forms) ----
+    ceiling = None
+    if rank == 0 and not args.no_ceiling:
+        ceiling = pruning_ceiling(weights, batch_ptrs, max_batch_bytes, forms["plain"]["threshold"],
+                                  forms["plain"]["decode_warps"], stream, torch)
+
     # ---- end to end through velo_run_host with host buffers (pruned form) ----
     e2e = run_e2e(args, chunks, plan, local_rank, torch, world, dist, forms["pruned"]["threshold"], weights,
                    forms["pruned"]["decode_warps"])
@@ -409,7 +492,9 @@ def run_ours(args, rank, world, local_rank):
         "config": {"workload": f"{WORKLOAD}: {n_events} events per GPU, pileup nu ~ U(2,20), seed 4, events "
                                f"rank*{n_events}..., MLP-pruned search; events above the scorer's trained "
                                f"occupancy fall back to the plain search", "events_per_gpu": n_events,
-                   "batch_events": BUCKET, "batches_per_step": n_batches, "mode": "pruned", "graphs": True,
+                   "batch_events": BUCKET, "batches_per_step": n_batches, "mode": "pruned",
+                   "graphs": f"{p['graphs']} CUDA graphs (one per batch-size bucket and stream), each serving every "
+                             f"batch of its bucket",
                    "streams": args.streams,
                    "scorer": scorer_info, "search_mapping": p["search_mapping"],
                    "decode_block": p["decode_block"],
@@ -425,6 +510,7 @@ def run_ours(args, rank, world, local_rank):
                   "gpu_launches": q["gpu_launches"]},
         "pruned_vs_plain": p["value"] / q["value"],
         "quality": quality,
+        "pruning_ceiling": ceiling,
         "e2e": e2e,
         "gpu_launches": p["gpu_launches"],
         "clocks": p["clocks"],
@@ -612,6 +698,70 @@ def pv_leg(batch, threshold):
     return out
 
 
+def stage_bytes(census, n_events):
+    """Algorithmic bytes of each stage for a pass with these totals (raw bytes, clusters,
+    tracks, track hits): what the stage must read and write at least."""
+    clusters, tracks, track_hits, raw_bytes = (census[k] for k in ("clusters", "tracks", "track_hits", "raw_bytes"))
+    return {
+        "decode_cluster_sort": raw_bytes + 16 * clusters + 8 * clusters,  # raw in, hits and windows out
+        "search_by_triplet": 16 * clusters + 8 * clusters + 2 * track_hits + 2 * tracks,
+        "event_scan": 16 * n_events,
+        "consolidate_fit": 34 * track_hits + 98 * tracks + 8 * tracks,
+    }
+
+
+def workload_leg(config, n_events, batch_sizes, threshold, decode_warps, threads, torch, first_event=0):
+    """The plain chain on another workload of the reference configuration list, device-resident,
+    in consecutive batches whose sizes cycle through `batch_sizes` (one CUDA graph per batch-size
+    bucket serves them all): events/s over one pass (CUDA events, one stream, after one untimed
+    pass), the graphs used, and each stage's time and algorithmic GB/s."""
+    chunks = [events.generate_config(config, n_events=min(CHUNK, n_events - a), first_event=first_event + a,
+                                     threads=threads, with_mc=False) for a in range(0, n_events, CHUNK)]
+    dev = torch.device("cuda")
+    d_raw = [torch.from_numpy(c.raw).to(dev) for c in chunks]
+    plan, keep = [], []
+    for ci, c in enumerate(chunks):
+        a, k = 0, 0
+        while a < c.n_events:
+            b = min(c.n_events, a + batch_sizes[k % len(batch_sizes)])
+            o = (c.offsets[a:b + 1] - c.offsets[a]).astype(np.uint64)
+            t = torch.from_numpy(o.view(np.int64)).to(dev)
+            keep.append(t)
+            plan.append((d_raw[ci].data_ptr() + int(c.offsets[a]), t.data_ptr(), b - a, int(o[-1])))
+            a, k = b, k + 1
+    vc = chain.VeloChain(max_events=max(batch_sizes), max_raw_bytes=max(p[3] for p in plan) + 4096, use_graphs=True)
+    vc.set_block_threshold(threshold)
+    vc.set_decode_warps(decode_warps)
+    s = torch.cuda.current_stream()
+    census = dict(clusters=0, tracks=0, track_hits=0, raw_bytes=sum(int(c.raw.size) for c in chunks))
+    for raw_p, off_p, n, _ in plan:  # untimed pass: graphs, census
+        vc.run_device(raw_p, off_p, n, s.cuda_stream)
+        t, h, c = vc.sync()
+        census["tracks"] += t
+        census["track_hits"] += h
+        census["clusters"] += c
+    vc.set_timing(True)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(s)
+    for raw_p, off_p, n, _ in plan:
+        vc.run_device(raw_p, off_p, n, s.cuda_stream)
+    end.record(s)
+    torch.cuda.synchronize()
+    ms = start.elapsed_time(end)
+    st = vc.stage_times()
+    runs = max(1, st.pop("runs"))
+    out = {"workload": config, "events": n_events, "batches": len(plan), "batch_sizes": list(batch_sizes),
+           "events_per_s": n_events / (ms / 1e3), "ms": ms, "graphs": vc.graph_count(),
+           "timing": "CUDA events around one pass after an untimed one, one stream",
+           "totals": census}
+    if runs >= len(plan):  # every launch's stage events kept: per-stage times and GB/s
+        alg = stage_bytes(census, n_events)
+        out["stage_ms"] = {k: v for k, v in st.items() if v > 0}
+        out["stage_gbs"] = {k: alg[k] / (st[k] / 1e3) / 1e9 for k in alg if st.get(k, 0) > 0}
+    vc.close()
+    return out
+
+
 # Algorithmic bytes of the global event cut per event: the SciFi and UT bank offset tables,
 # the hit-count word of each UT bank, and the outputs (two counts, a flag, a list entry).
 def gec_bytes(ut, sf):
@@ -726,6 +876,11 @@ def main():
     ap.add_argument("--weights", default=None, help="scorer weights (default: the committed file)")
     ap.add_argument("--retrain", action="store_true", help="train the scorer here instead of loading it")
     ap.add_argument("--no-extras", action="store_true", help="skip the CPU baseline and reference-GPU legs")
+    ap.add_argument("--no-ceiling", action="store_true", help="skip the per-stage / pruning-ceiling leg")
+    ap.add_argument("--batched-events", type=int, default=500_000,
+                    help="events of the nu ~ U(2,15) leg in 1k/4k/16k-event batches (0: skip)")
+    ap.add_argument("--high-occ-events", type=int, default=200_000,
+                    help="events of the nu = 15, 10%% noisy leg (0: skip)")
     args = ap.parse_args()
     BUCKET, CHUNK = args.batch, 4 * args.batch
     rank = int(os.environ.get("RANK", "0"))
@@ -764,6 +919,18 @@ def main():
                                       result["config"]["search_mapping"]["block_above_clusters"])
             except Exception as ex:
                 result["pv"] = {"error": str(ex)}
+            for key, cfg_name, n_ev, sizes in (("batched_500k", "batched_500k", args.batched_events,
+                                                 (1000, 4000, 16000)),
+                                                ("high_occupancy_200k", "high_occupancy_200k", args.high_occ_events,
+                                                 (BUCKET,))):
+                if n_ev <= 0:
+                    continue
+                try:
+                    import torch
+                    result[key] = workload_leg(cfg_name, n_ev, sizes, result["config"]["search_mapping"]["block_above_clusters"],
+                                               result["config"]["decode_block"]["warps"], threads, torch)
+                except Exception as ex:
+                    result[key] = {"error": str(ex)}
             try:
                 result["global_event_cut"] = gec_leg(chunks[0].subset(0, min(SIDE_BATCH, chunks[0].n_events)),
                                                      result["config"]["search_mapping"]["block_above_clusters"],

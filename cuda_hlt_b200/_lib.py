@@ -102,6 +102,7 @@ class VeloOutputs(C.Structure):
         ("n_selected", C.c_void_p),
         ("gec_counts", C.c_void_p),
         ("gec_flags", C.c_void_p),
+        ("hit_windows", C.c_void_p),
     ]
 
 
@@ -137,6 +138,10 @@ GPU_SYMBOLS = [
     "velo_create",
     "velo_run",
     "velo_run_host",
+    "velo_run_u32",
+    "velo_run_host_u32",
+    "velo_run_selected_u32",
+    "velo_graph_count",
     "velo_run_gec",
     "velo_run_gec_host",
     "velo_sync",
@@ -153,6 +158,7 @@ GPU_SYMBOLS = [
     "velo_search_static",
     "velo_version",
     "velo_set_mode",
+    "velo_capture_labels",
     "velo_set_pv",
     "velo_mlp_trainer_create",
     "velo_mlp_trainer_destroy",
@@ -225,6 +231,14 @@ def gpu_lib():
         lib.velo_run.restype = C.c_int
         lib.velo_run_host.argtypes = [P, P, P, C.c_uint32, P, C.POINTER(VeloOutputs)]
         lib.velo_run_host.restype = C.c_int
+        lib.velo_run_u32.argtypes = [P, P, P, C.c_uint32, P, C.POINTER(VeloOutputs)]
+        lib.velo_run_u32.restype = C.c_int
+        lib.velo_run_host_u32.argtypes = [P, P, P, C.c_uint32, P, C.POINTER(VeloOutputs)]
+        lib.velo_run_host_u32.restype = C.c_int
+        lib.velo_run_selected_u32.argtypes = [P, P, P, C.c_uint32, P, C.c_uint32, P, C.POINTER(VeloOutputs)]
+        lib.velo_run_selected_u32.restype = C.c_int
+        lib.velo_graph_count.argtypes = [P, C.POINTER(C.c_uint32)]
+        lib.velo_graph_count.restype = C.c_int
         lib.velo_run_gec.argtypes = [P, P, P, C.POINTER(VeloGecInput), C.c_uint32, P, C.POINTER(VeloOutputs)]
         lib.velo_run_gec.restype = C.c_int
         lib.velo_run_gec_host.argtypes = [P, P, P, C.POINTER(VeloGecInput), C.c_uint32, P, C.POINTER(VeloOutputs)]
@@ -255,6 +269,8 @@ def gpu_lib():
         lib.velo_search_static.restype = C.c_int
         lib.velo_version.argtypes = []
         lib.velo_version.restype = C.c_char_p
+        lib.velo_capture_labels.argtypes = [P, C.c_int, C.c_uint32]
+        lib.velo_capture_labels.restype = C.c_int
         lib.velo_set_mode.argtypes = [P, C.c_uint32]
         lib.velo_set_mode.restype = C.c_int
         lib.velo_set_pv.argtypes = [P, C.c_int]

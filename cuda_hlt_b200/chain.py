@@ -38,7 +38,7 @@ PV_MAX_VERTICES = 32
 PV_VERTEX = np.dtype([("x", "<f4"), ("y", "<f4"), ("z", "<f4"), ("chi2", "<f4"), ("ndof", "<i4"), ("n_tracks", "<u4"),
                       ("cov00", "<f4"), ("cov10", "<f4"), ("cov11", "<f4"), ("cov20", "<f4"), ("cov21", "<f4"),
                       ("cov22", "<f4"), ("n_tracks_unused", "<i4")])
-MODE_PLAIN, MODE_PRUNED = 0, 1
+MODE_PLAIN, MODE_PRUNED, MODE_LABELS = 0, 1, 2
 MAP_AUTO, MAP_BLOCK, MAP_WARP = 0, 1, 2
 N_MODULES = 52
 STATE_FIELDS = ("x", "y", "tx", "ty", "c00", "c20", "c22", "c11", "c31", "c33", "chi2", "z")
@@ -111,6 +111,25 @@ class VeloChain:
         _check(self.lib.velo_run_host(self.ctx, batch.raw.ctypes.data, batch.offsets.ctypes.data, batch.n_events,
                                       C.c_void_p(stream), C.byref(self.out)), "velo_run_host")
 
+    def run_host_u32(self, raw, offsets32, stream=0):
+        """Host batch with u32 byte offsets (the reference's input format): raw uint8 array,
+        offsets32 uint32 array of n_events + 1 entries."""
+        offsets32 = np.ascontiguousarray(offsets32, np.uint32)
+        self.n_events = len(offsets32) - 1
+        _check(self.lib.velo_run_host_u32(self.ctx, raw.ctypes.data, offsets32.ctypes.data, self.n_events,
+                                          C.c_void_p(stream), C.byref(self.out)), "velo_run_host_u32")
+
+    def run_device_u32(self, raw_ptr, offsets32_ptr, n_events, stream=0):
+        """Device-resident input with u32 offsets[n+1]."""
+        self.n_events = n_events
+        _check(self.lib.velo_run_u32(self.ctx, C.c_void_p(raw_ptr), C.c_void_p(offsets32_ptr), n_events,
+                                     C.c_void_p(stream), C.byref(self.out)), "velo_run_u32")
+
+    def graph_count(self):
+        n = C.c_uint32()
+        _check(self.lib.velo_graph_count(self.ctx, C.byref(n)), "velo_graph_count")
+        return n.value
+
     def run_device(self, raw_ptr, offsets_ptr, n_events, stream=0):
         """Runs on device-resident input (raw bytes, u64 offsets[n+1])."""
         self.n_events = n_events
@@ -161,8 +180,14 @@ class VeloChain:
         _check(self.lib.velo_set_pv(self.ctx, int(bool(enabled))), "velo_set_pv")
 
     def set_mode(self, mode):
-        """MODE_PLAIN (reference semantics) or MODE_PRUNED (learned scorer, set_mlp first)."""
+        """MODE_PLAIN (reference semantics), MODE_PRUNED (learned scorer, set_mlp first) or
+        MODE_LABELS (the plain search's own labels, capture_labels first)."""
         _check(self.lib.velo_set_mode(self.ctx, int(mode)), "velo_set_mode")
+
+    def capture_labels(self, ext=False, max_event_clusters=0xFFFFFFFF):
+        """After a plain run (and sync): keeps the plain search's labels of every hit for
+        runs in MODE_LABELS on the same batch (a perfect scorer; velo_capture_labels)."""
+        _check(self.lib.velo_capture_labels(self.ctx, int(bool(ext)), int(max_event_clusters)), "velo_capture_labels")
 
     def set_mlp(self, weights):
         """Loads a VeloMlpWeights (see cuda_hlt_b200.mlp) for the pruned mode."""

@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstring>
 #include <array>
+#include <list>
 #include <map>
 #include <tuple>
 #include <vector>
@@ -44,10 +45,18 @@ struct VeloCtx {
   float* d_mlp_norm = nullptr;
   MlpDevice mlp{};
   bool mlp_loaded = false;
+  // labels of a plain run kept by velo_capture_labels (VELO_MODE_LABELS)
+  uint8_t* d_labels = nullptr;
+  bool labels_ready = false;
+  uint32_t labels_ext = 0;
+  uint32_t labels_max_hits = 0;
   uint32_t mode = VELO_MODE_PLAIN;
-  // input staging (for velo_run_host)
+  // input staging (for velo_run_host / velo_run_host_u32)
   uint8_t* d_raw = nullptr;
   uint64_t* d_raw_offsets = nullptr;
+  uint32_t* d_raw_offsets32 = nullptr;
+  // the parameters of the current run, read by the kernels (set_run_kernel)
+  RunParams* d_run = nullptr;
   // work buffers
   float4* d_hxyzp = nullptr;
   uint32_t* d_hid = nullptr;
@@ -89,8 +98,9 @@ struct VeloCtx {
   uint32_t last_n = 0;
   uint32_t launches = 0;
   bool timing = false;
-  // Stage timing: one set of kStageEvents events per launch sequence; a graph keeps the set
-  // it was captured with, plain launches cycle through the sets.
+  // Stage timing: one set of kStageEvents events per launch sequence, taken in turn from a
+  // pool of kEventSets sets by plain launches and graph launches alike (a graph's event-record
+  // nodes are pointed at the set before it is launched).
   // Events 0..6 bound the six chain stages in order; 7 and 8 bound the global event cut
   // (recorded back to back when it does not run).
   static constexpr int kStageEvents = 9;
@@ -100,29 +110,27 @@ struct VeloCtx {
   int ev_current = -1;
   int decode_warps = 8;
   int search_wpb = 4;
-  uint32_t decode_blocks = 0, search_blocks = 0, search_block_blocks = 0, fill_blocks = 0, fill_pruned_blocks = 0,
+  uint32_t decode_blocks = 0, search_blocks = 0, search_block_blocks = 0, fill_blocks = 0,
            feature_blocks = 0, score_blocks = 0;
-  // CUDA graphs per (n_events, raw, offsets, stream, global event cut inputs)
+  // CUDA graphs per (batch-size bucket, stream, global event cut on or off): the kernels read
+  // the run's inputs from d_run, so a graph serves every batch of its bucket; at most
+  // kMaxGraphs are kept, the least recently launched evicted first
+  static constexpr size_t kMaxGraphs = 16;
   struct GraphKey {
-    uint32_t n;
-    const void* raw;
-    const void* offsets;
+    uint32_t bucket;
     cudaStream_t stream;
-    const void* ut = nullptr;
-    const void* ut_offsets = nullptr;
-    const void* scifi = nullptr;
-    const void* scifi_offsets = nullptr;
-    uint32_t gec_max = 0;
-    bool operator<(const GraphKey& o) const
-    {
-      return std::tie(n, raw, offsets, stream, ut, ut_offsets, scifi, scifi_offsets, gec_max) <
-             std::tie(o.n, o.raw, o.offsets, o.stream, o.ut, o.ut_offsets, o.scifi, o.scifi_offsets, o.gec_max);
-    }
+    bool gec;
+    bool operator<(const GraphKey& o) const { return std::tie(bucket, stream, gec) < std::tie(o.bucket, o.stream, o.gec); }
   };
   struct GraphEntry {
     cudaGraphExec_t exec;
-    int ev_set;  // event set recorded by the graph, -1 without timing
+    cudaGraph_t graph;  // kept: its event-record nodes are rebound before each timed launch
+    std::array<cudaGraphNode_t, kStageEvents> ev_nodes;  // event-record node of each stage event
+    bool timed;         // captured with the stage events
+    uint32_t launches;  // kernels in the graph
+    std::list<GraphKey>::iterator lru;
   };
+  std::list<GraphKey> lru;  // most recently launched first
   std::map<GraphKey, GraphEntry> graphs;
 };
 
@@ -148,7 +156,7 @@ cudaError_t dalloc(T*& p, size_t count)
 
 void free_all(VeloCtx* c)
 {
-  void* ptrs[] = {c->d_geometry, c->d_sp_patterns, c->d_sp_fx, c->d_sp_fy, c->d_sp_sizes, c->d_mlp_w, c->d_mlp_norm,
+  void* ptrs[] = {c->d_labels, c->d_geometry, c->d_sp_patterns, c->d_sp_fx, c->d_sp_fy, c->d_sp_sizes, c->d_mlp_w, c->d_mlp_norm,
                   c->d_hit_size, c->d_windows, c->d_keep, c->d_cand_feat, c->d_cand_slot, c->d_cand_rec, c->d_raw, c->d_raw_offsets, c->d_hxyzp,
                   c->d_hid, c->d_stage_xyzp, c->d_stage_id, c->d_module_start, c->d_module_num, c->d_event_hit_base,
                   c->d_event_hits, c->d_status, c->d_track_n, c->d_track_hits, c->d_tracklets, c->d_weak, c->d_ttf,
@@ -161,14 +169,19 @@ void free_all(VeloCtx* c)
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c->h_totals) cudaFreeHost(c->h_totals);
-  for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second.exec);
+  for (auto& kv : c->graphs) {
+    cudaGraphExecDestroy(kv.second.exec);
+    cudaGraphDestroy(kv.second.graph);
+  }
+  if (c->d_run) cudaFree(c->d_run);
+  if (c->d_raw_offsets32) cudaFree(c->d_raw_offsets32);
   for (auto& set : c->ev_sets)
     for (auto& e : set)
       if (e) cudaEventDestroy(e);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
 }
 
-constexpr uint32_t kPlainEventSets = 8;
+constexpr uint32_t kEventSets = 64;  // launch sequences whose stage times are kept
 
 int add_event_set(VeloCtx* c)
 {
@@ -180,12 +193,13 @@ int add_event_set(VeloCtx* c)
   return static_cast<int>(c->ev_sets.size() - 1);
 }
 
-ChainPointers pointers(VeloCtx* c, const void* raw, const uint64_t* offsets, uint32_t n)
+// Kernel parameters of a run whose grids are sized for n_grid events (the run's own inputs
+// and count are in c->d_run).
+ChainPointers pointers(VeloCtx* c, uint32_t n_grid)
 {
   ChainPointers P{};
-  P.raw = static_cast<const uint8_t*>(raw);
-  P.raw_offsets = offsets;
-  P.n_events = n;
+  P.run = c->d_run;
+  P.n_grid = n_grid;
   P.k = DeviceConstants{reinterpret_cast<const float*>(c->d_geometry), c->d_sp_patterns, c->d_sp_fx, c->d_sp_fy,
                         c->d_sp_sizes};
   P.hits = HitsAoS{c->d_hxyzp, c->d_hid};
@@ -197,7 +211,7 @@ ChainPointers pointers(VeloCtx* c, const void* raw, const uint64_t* offsets, uin
   P.status = c->d_status;
   P.hit_size = c->d_hit_size;
   P.windows = c->d_windows;
-  P.keep = c->mode == VELO_MODE_PRUNED ? c->d_keep : nullptr;
+  P.keep = c->mode == VELO_MODE_PRUNED ? c->d_keep : (c->mode == VELO_MODE_LABELS ? c->d_labels : nullptr);
   P.cand_feat = c->d_cand_feat;
   P.cand_slot = c->d_cand_slot;
   P.cand_rec = c->d_cand_rec;
@@ -219,7 +233,66 @@ ChainPointers pointers(VeloCtx* c, const void* raw, const uint64_t* offsets, uin
   P.block_events = c->d_block_events;
   P.block_threshold = c->block_threshold;
   P.mlp = c->mlp;
+  if (c->mode == VELO_MODE_LABELS) {
+    P.mlp = MlpDevice{};
+    P.mlp.use_ext = c->labels_ext;
+    P.mlp.max_hits = c->labels_max_hits;
+  }
   return P;
+}
+
+// Labels of the hits of one run's events from the tracks of its plain search, one block per
+// event: bit 0 on a final track, bit 1 the fourth or a later hit of one (the labels the
+// scorer is trained on). Events above `max_hits` clusters get every bit set (nothing pruned).
+__global__ void __launch_bounds__(256) capture_labels_kernel(ChainPointers P, uint8_t* labels, uint32_t max_hits)
+{
+  const uint32_t n_events = P.run->n_events;
+  for (uint32_t e = blockIdx.x; e < n_events; e += gridDim.x) {
+    const uint32_t nhits = P.event_hits[e], base = P.event_hit_base[e], status = P.status[e];
+    const bool runnable = !(status & (kStatusBadRawEvent | kStatusHitOverflow)) && nhits <= kEventHitCap && nhits > 0;
+    if (!runnable) continue;
+    uint8_t* L = labels + base;
+    const bool all = nhits > max_hits;
+    for (uint32_t h = threadIdx.x; h < nhits; h += blockDim.x) L[h] = all ? 3u : 0u;
+    __syncthreads();
+    if (!all) {
+      const uint32_t nt = min(P.event_tracks[e], kMaxTracks);  // a hit is on one track at most
+      const uint16_t* tn = P.scratch.track_n + static_cast<size_t>(e) * kMaxTracks;
+      const uint16_t* th = P.scratch.track_hits + static_cast<size_t>(e) * kMaxTracks * kMaxTrackSize;
+      for (uint32_t t = threadIdx.x; t < nt; t += blockDim.x) {
+        const uint32_t n = tn[t];
+        for (uint32_t k = 0; k < n; ++k) L[th[t * kMaxTrackSize + k]] = k >= 3 ? 3u : 1u;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// VELO_MODE_LABELS: seeds without the "on a final track" label lose their h0 window, as the
+// scorer's pruned seeds do; the search reads the labels as extension-keep bits.
+__global__ void __launch_bounds__(kFillThreads) label_seeds_kernel(ChainPointers P)
+{
+  const uint32_t n_events = P.run->n_events;
+  for (uint32_t e = blockIdx.x; e < n_events; e += gridDim.x) {
+    const uint32_t nhits = P.event_hits[e], base = P.event_hit_base[e], status = P.status[e];
+    const bool runnable = !(status & (kStatusBadRawEvent | kStatusHitOverflow)) && nhits <= kEventHitCap && nhits > 0;
+    if (!runnable) continue;
+    if (nhits > P.mlp.max_hits) {
+      if (threadIdx.x == 0) P.status[e] = status | kStatusMlpFallback;
+      continue;
+    }
+    const uint32_t lo = P.module_start[e * kModules + 2] - base, hi = P.module_start[e * kModules + 50] - base;
+    for (uint32_t h = lo + threadIdx.x; h < hi; h += blockDim.x)
+      if (!(P.keep[base + h] & 1u)) P.windows[base + h].x = 0xFFFFFFFFu;
+  }
+}
+
+// Writes the parameters of the next run where the kernels read them and clears the work
+// queues. Launched on the run's stream before the chain (or its graph), outside any capture.
+__global__ void set_run_kernel(RunParams* dst, RunParams v, uint32_t* queue)
+{
+  if (threadIdx.x == 0) *dst = v;
+  if (threadIdx.x < 8) queue[threadIdx.x] = 0u;
 }
 
 // Inside a stream capture an event record must be marked external to become a node that
@@ -231,9 +304,8 @@ cudaError_t record(cudaEvent_t e, cudaStream_t s, bool capturing)
 
 int launch_chain(VeloCtx* c, const ChainPointers& P, const GecPointers* G, cudaStream_t s, bool capturing = false)
 {
-  const uint32_t n = P.n_events;
+  const uint32_t n = P.n_grid;
   c->launches = 0;
-  VCK(cudaMemsetAsync(c->d_queue, 0, 8 * sizeof(uint32_t), s));
   if (c->timing && c->ev_current >= 0) VCK(record(c->ev_sets[c->ev_current][7], s, capturing));
   if (G) {  // global event cut: the event list decode reads
     const uint32_t blocks = std::min<uint32_t>((n + kGecThreads / 32 - 1) / (kGecThreads / 32), c->gec_blocks);
@@ -245,26 +317,30 @@ int launch_chain(VeloCtx* c, const ChainPointers& P, const GecPointers* G, cudaS
   }
   if (c->timing && c->ev_current >= 0) VCK(record(c->ev_sets[c->ev_current][8], s, capturing));
   if (c->timing && c->ev_current >= 0) VCK(record(c->ev_sets[c->ev_current][0], s, capturing));
+  const bool pruned = c->mode == VELO_MODE_PRUNED;
   {
     const uint32_t blocks = std::min<uint32_t>(n, c->decode_blocks);
-    if (c->decode_warps == 8)
-      decode_cluster_sort_kernel<8><<<blocks, 256, 0, s>>>(P);
-    else
-      decode_cluster_sort_kernel<4><<<blocks, 128, 0, s>>>(P);
+    // the decode kernel also computes the phi windows (fill_candidates) and, in the pruned
+    // mode, the scorer's candidate list
+    if (c->decode_warps == 8) {
+      if (pruned) decode_cluster_sort_kernel<8, true><<<blocks, 256, 0, s>>>(P);
+      else decode_cluster_sort_kernel<8, false><<<blocks, 256, 0, s>>>(P);
+    } else {
+      if (pruned) decode_cluster_sort_kernel<4, true><<<blocks, 128, 0, s>>>(P);
+      else decode_cluster_sort_kernel<4, false><<<blocks, 128, 0, s>>>(P);
+    }
     VCK(cudaGetLastError());
     ++c->launches;
   }
   if (c->timing && c->ev_current >= 0) VCK(record(c->ev_sets[c->ev_current][1], s, capturing));
-  if (P.keep) {
-    fill_candidates_kernel<true><<<std::min<uint32_t>(n, c->fill_pruned_blocks), kFillThreads, 0, s>>>(P);
-    VCK(cudaGetLastError());
+  if (c->mode == VELO_MODE_LABELS) {
+    label_seeds_kernel<<<std::min<uint32_t>(n, c->fill_blocks), kFillThreads, 0, s>>>(P);
+    ++c->launches;
+  } else if (pruned) {
     candidate_features_kernel<<<c->feature_blocks, kFillThreads, 0, s>>>(P);
     VCK(cudaGetLastError());
     score_candidates_kernel<<<c->score_blocks, kMlpTile, kScoreSmem, s>>>(P);
-    c->launches += 3;
-  } else {
-    fill_candidates_kernel<false><<<std::min<uint32_t>(n, c->fill_blocks), kFillThreads, 0, s>>>(P);
-    ++c->launches;
+    c->launches += 2;
   }
   VCK(cudaGetLastError());
   if (c->timing && c->ev_current >= 0) VCK(record(c->ev_sets[c->ev_current][2], s, capturing));
@@ -309,9 +385,9 @@ void size_decode_grid(VeloCtx* c)
 {
   int occ = 0;
   if (c->decode_warps == 8)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, decode_cluster_sort_kernel<8>, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, decode_cluster_sort_kernel<8, true>, 256, 0);
   else
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, decode_cluster_sort_kernel<4>, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, decode_cluster_sort_kernel<4, true>, 128, 0);
   c->decode_blocks = static_cast<uint32_t>(std::max(1, occ) * c->sm_count);
 }
 
@@ -332,8 +408,20 @@ void drop_graphs(VeloCtx* c)
 {
   cudaSetDevice(c->device);
   cudaDeviceSynchronize();
-  for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second.exec);
+  for (auto& kv : c->graphs) {
+    cudaGraphExecDestroy(kv.second.exec);
+    cudaGraphDestroy(kv.second.graph);
+  }
   c->graphs.clear();
+  c->lru.clear();
+}
+
+// Batch-size bucket of a graph: 1,024 events times a power of 4, at most the context's size.
+uint32_t bucket_of(const VeloCtx* c, uint32_t n)
+{
+  uint64_t b = 1024;
+  while (b < n) b *= 4;
+  return static_cast<uint32_t>(std::min<uint64_t>(b, c->cfg.max_events));
 }
 
 }  // namespace
@@ -374,6 +462,8 @@ int velo_create(const VeloConfig* cfg, const void* geometry, size_t geometry_byt
   ok &= dalloc(c->d_mlp_norm, 32) == cudaSuccess;
   ok &= dalloc(c->d_raw, cfg->max_raw_bytes + 16) == cudaSuccess;
   ok &= dalloc(c->d_raw_offsets, N + 1) == cudaSuccess;
+  ok &= dalloc(c->d_raw_offsets32, N + 1) == cudaSuccess;
+  ok &= dalloc(c->d_run, 1) == cudaSuccess;
   ok &= dalloc(c->d_hxyzp, c->hit_capacity) == cudaSuccess;
   ok &= dalloc(c->d_hid, c->hit_capacity) == cudaSuccess;
   ok &= dalloc(c->d_stage_xyzp, 2 * c->hit_capacity) == cudaSuccess;
@@ -438,10 +528,8 @@ int velo_create(const VeloConfig* cfg, const void* geometry, size_t geometry_byt
                        static_cast<int>(kStageCap * sizeof(float4)));
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, search_block_kernel, kBlockThreads, kStageCap * sizeof(float4));
   c->search_block_blocks = static_cast<uint32_t>(std::max(1, occ) * c->sm_count);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fill_candidates_kernel<false>, kFillThreads, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, label_seeds_kernel, kFillThreads, 0);
   c->fill_blocks = static_cast<uint32_t>(std::max(1, occ) * c->sm_count);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fill_candidates_kernel<true>, kFillThreads, 0);
-  c->fill_pruned_blocks = static_cast<uint32_t>(std::max(1, occ) * c->sm_count);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, candidate_features_kernel, kFillThreads, 0);
   c->feature_blocks = static_cast<uint32_t>(std::max(1, occ) * c->sm_count);
   // the scorer: as many CTAs per SM as shared memory holds (1 KB of it is reserved per
@@ -478,7 +566,8 @@ static int fill_outputs(VeloCtx* c, uint32_t n, VeloOutputs* out)
   out->hit_id = c->d_hid;
   out->hit_capacity = c->hit_capacity;
   out->hit_size = c->d_hit_size;
-  out->hit_keep = c->mode == VELO_MODE_PRUNED ? c->d_keep : nullptr;
+  out->hit_windows = reinterpret_cast<uint32_t*>(c->d_windows);
+  out->hit_keep = c->mode == VELO_MODE_PRUNED ? c->d_keep : (c->mode == VELO_MODE_LABELS ? c->d_labels : nullptr);
   if (c->pv) {
     out->pv_vertices = c->d_pv_vertices;
     out->pv_count = c->d_pv_count;
@@ -488,15 +577,18 @@ static int fill_outputs(VeloCtx* c, uint32_t n, VeloOutputs* out)
   return 0;
 }
 
-// velo_run with or without the global event cut in front (gec: device inputs, or null).
-static int run_chain(VeloCtx* c, const void* raw, const uint64_t* raw_offsets, const VeloGecInput* gec,
-                     uint32_t n_events, void* stream, VeloOutputs* out)
+// velo_run with or without the global event cut in front (gec: device inputs, or null), raw
+// offsets as u64 (raw_offsets) or u32 (raw_offsets32).
+static int run_chain(VeloCtx* c, const void* raw, const uint64_t* raw_offsets, const uint32_t* raw_offsets32,
+                     const VeloGecInput* gec, uint32_t n_events, void* stream, VeloOutputs* out,
+                     const uint32_t* event_list = nullptr, uint32_t n_raw = 0)
 {
-  if (!c || (!raw && n_events) || (!raw_offsets && n_events)) return VELO_ERR_INVALID;
+  if (!c || (!raw && n_events) || (!raw_offsets && !raw_offsets32 && n_events)) return VELO_ERR_INVALID;
   if (gec && n_events && (!gec->ut_raw || !gec->ut_offsets || !gec->scifi_raw || !gec->scifi_offsets))
     return VELO_ERR_INVALID;
   if (n_events > c->cfg.max_events) return VELO_ERR_CAPACITY;
   if (c->mode == VELO_MODE_PRUNED && !c->mlp_loaded) return VELO_ERR_STATE;
+  if (c->mode == VELO_MODE_LABELS && !c->labels_ready) return VELO_ERR_STATE;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (cudaSetDevice(c->device) != cudaSuccess) return VELO_ERR_CUDA;
   c->last_stream = s;
@@ -515,40 +607,52 @@ static int run_chain(VeloCtx* c, const void* raw, const uint64_t* raw_offsets, c
     if (gec) VCK(cudaMemsetAsync(c->d_n_selected, 0, sizeof(uint32_t), s));
     return 0;
   }
-  ChainPointers P = pointers(c, raw, raw_offsets, n_events);
+  // the run's inputs, where the kernels read them
+  RunParams v{};
+  v.raw = static_cast<const uint8_t*>(raw);
+  v.raw_offsets = raw_offsets;
+  v.raw_offsets32 = raw_offsets ? nullptr : raw_offsets32;
+  v.n_events = n_events;
+  v.event_list = event_list;
+  v.n_raw = n_raw;
+  if (gec) {
+    v.gec_max = gec->max_clusters;
+    v.ut_raw = static_cast<const uint8_t*>(gec->ut_raw);
+    v.ut_offsets = gec->ut_offsets;
+    v.scifi_raw = static_cast<const uint8_t*>(gec->scifi_raw);
+    v.scifi_offsets = gec->scifi_offsets;
+  }
+  set_run_kernel<<<1, 32, 0, s>>>(c->d_run, v, c->d_queue);
+  VCK(cudaGetLastError());
+  const uint32_t n_grid = c->cfg.use_graphs ? bucket_of(c, n_events) : n_events;
+  ChainPointers P = pointers(c, n_grid);
   GecPointers G{};
   if (gec) {
-    G = GecPointers{static_cast<const uint8_t*>(gec->ut_raw), gec->ut_offsets,
-                    static_cast<const uint8_t*>(gec->scifi_raw), gec->scifi_offsets, n_events, gec->max_clusters,
-                    c->d_gec_counts, c->d_gec_flags, c->d_event_list, c->d_n_selected};
+    G = GecPointers{c->d_run, c->d_gec_counts, c->d_gec_flags, c->d_event_list, c->d_n_selected};
     P.event_list = c->d_event_list;
     P.n_selected = c->d_n_selected;
   }
   const GecPointers* Gp = gec ? &G : nullptr;
   if (c->cfg.use_graphs) {
-    VeloCtx::GraphKey key{n_events, raw, raw_offsets, s};
-    if (gec) {
-      key.ut = gec->ut_raw;
-      key.ut_offsets = gec->ut_offsets;
-      key.scifi = gec->scifi_raw;
-      key.scifi_offsets = gec->scifi_offsets;
-      key.gec_max = gec->max_clusters;
-    }
+    const VeloCtx::GraphKey key{n_grid, s, gec != nullptr};
     auto it = c->graphs.find(key);
     if (it == c->graphs.end()) {
+      if (c->graphs.size() >= VeloCtx::kMaxGraphs) {  // evict the least recently launched
+        auto old = c->graphs.find(c->lru.back());
+        VCK(cudaStreamSynchronize(old->first.stream));
+        cudaGraphExecDestroy(old->second.exec);
+        cudaGraphDestroy(old->second.graph);
+        c->lru.pop_back();
+        c->graphs.erase(old);
+      }
       cudaStream_t cap = s;
       bool tmp = false;
       if (cap == nullptr) {  // the legacy default stream cannot be captured
         VCK(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
         tmp = true;
       }
-      int set = -1;
-      if (c->timing) {
-        const int rc = add_event_set(c);
-        if (rc < 0) return rc;
-        set = rc;
-      }
-      c->ev_current = set;
+      // with timing on, the capture records set 0's events: they only mark the nodes
+      c->ev_current = c->timing ? 0 : -1;
       cudaGraph_t g;
       VCK(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
       const int rc = launch_chain(c, P, Gp, cap, true);
@@ -556,35 +660,80 @@ static int run_chain(VeloCtx* c, const void* raw, const uint64_t* raw_offsets, c
       if (tmp) cudaStreamDestroy(cap);
       if (rc != 0) return rc;
       VCK(ce);
-      cudaGraphExec_t exec;
-      VCK(cudaGraphInstantiate(&exec, g, 0));
-      cudaGraphDestroy(g);
-      it = c->graphs.emplace(key, VeloCtx::GraphEntry{exec, set}).first;
+      VeloCtx::GraphEntry entry{};
+      entry.graph = g;
+      entry.timed = c->timing;
+      entry.launches = c->launches;
+      if (entry.timed) {
+        size_t nn = 0;
+        VCK(cudaGraphGetNodes(g, nullptr, &nn));
+        std::vector<cudaGraphNode_t> nodes(nn);
+        VCK(cudaGraphGetNodes(g, nodes.data(), &nn));
+        for (cudaGraphNode_t node : nodes) {
+          cudaGraphNodeType type;
+          VCK(cudaGraphNodeGetType(node, &type));
+          if (type != cudaGraphNodeTypeEventRecord) continue;
+          cudaEvent_t ev;
+          VCK(cudaGraphEventRecordNodeGetEvent(node, &ev));
+          for (int i = 0; i < VeloCtx::kStageEvents; ++i)
+            if (c->ev_sets[0][i] == ev) entry.ev_nodes[i] = node;
+        }
+      }
+      VCK(cudaGraphInstantiate(&entry.exec, g, 0));
+      c->lru.push_front(key);
+      entry.lru = c->lru.begin();
+      it = c->graphs.emplace(key, entry).first;
+    } else {
+      c->lru.splice(c->lru.begin(), c->lru, it->second.lru);
+    }
+    if (c->timing && it->second.timed) {
+      // this launch records into the next set of the pool
+      const int k = static_cast<int>(c->ev_next++ % kEventSets);
+      for (int i = 0; i < VeloCtx::kStageEvents; ++i)
+        if (it->second.ev_nodes[i]) VCK(cudaGraphExecEventRecordNodeSetEvent(it->second.exec, it->second.ev_nodes[i],
+                                                                          c->ev_sets[k][i]));
+      c->ev_used[k] = 1;
     }
     VCK(cudaGraphLaunch(it->second.exec, s));
-    if (it->second.ev_set >= 0) c->ev_used[it->second.ev_set] = 1;
+    c->launches = it->second.launches + 1;  // the graph's kernels and set_run_kernel
     return 0;
   }
   c->ev_current = -1;
   if (c->timing) {
-    // plain launches cycle through the first kPlainEventSets sets
-    c->ev_current = static_cast<int>(c->ev_next++ % kPlainEventSets);
+    c->ev_current = static_cast<int>(c->ev_next++ % kEventSets);
     c->ev_used[c->ev_current] = 1;
   }
-  return launch_chain(c, P, Gp, s);
+  const int rc = launch_chain(c, P, Gp, s);
+  ++c->launches;  // set_run_kernel
+  return rc;
 }
 
 int velo_run(VeloCtx* c, const void* raw, const uint64_t* raw_offsets, uint32_t n_events, void* stream,
              VeloOutputs* out)
 {
-  return run_chain(c, raw, raw_offsets, nullptr, n_events, stream, out);
+  if (!raw_offsets && n_events) return VELO_ERR_INVALID;
+  return run_chain(c, raw, raw_offsets, nullptr, nullptr, n_events, stream, out);
+}
+
+int velo_run_u32(VeloCtx* c, const void* raw, const uint32_t* raw_offsets, uint32_t n_events, void* stream,
+                 VeloOutputs* out)
+{
+  if (!raw_offsets && n_events) return VELO_ERR_INVALID;
+  return run_chain(c, raw, nullptr, raw_offsets, nullptr, n_events, stream, out);
+}
+
+int velo_run_selected_u32(VeloCtx* c, const void* raw, const uint32_t* raw_offsets, uint32_t n_raw,
+                          const uint32_t* event_list, uint32_t n_events, void* stream, VeloOutputs* out)
+{
+  if ((!raw_offsets || !event_list) && n_events) return VELO_ERR_INVALID;
+  return run_chain(c, raw, nullptr, raw_offsets, nullptr, n_events, stream, out, event_list, n_raw);
 }
 
 int velo_run_gec(VeloCtx* c, const void* raw, const uint64_t* raw_offsets, const VeloGecInput* gec,
                  uint32_t n_events, void* stream, VeloOutputs* out)
 {
-  if (!gec) return VELO_ERR_INVALID;
-  return run_chain(c, raw, raw_offsets, gec, n_events, stream, out);
+  if (!gec || (!raw_offsets && n_events)) return VELO_ERR_INVALID;
+  return run_chain(c, raw, raw_offsets, nullptr, gec, n_events, stream, out);
 }
 
 // Copies a host batch (bytes from offsets[0] to offsets[n], offsets[n + 1]) to device buffers,
@@ -642,7 +791,39 @@ int velo_run_gec_host(VeloCtx* c, const void* raw_host, const uint64_t* raw_offs
   if (rc) return rc;
   const VeloGecInput dev{c->d_gec_ut, c->d_gec_ut_offsets, c->d_gec_scifi, c->d_gec_scifi_offsets,
                          gec_host->max_clusters};
-  return run_chain(c, c->d_raw, c->d_raw_offsets, &dev, n_events, stream, out);
+  return run_chain(c, c->d_raw, c->d_raw_offsets, nullptr, &dev, n_events, stream, out);
+}
+
+// Copies a host batch with u32 offsets (bytes from offsets[0] to offsets[n]) to the
+// context's device buffers, rebasing the offsets when the batch does not start at byte 0.
+static int upload_batch_u32(VeloCtx* c, const void* raw_host, const uint32_t* offsets_host, uint32_t n, cudaStream_t s)
+{
+  const uint32_t first = offsets_host[0];
+  const uint64_t bytes = static_cast<uint64_t>(offsets_host[n]) - first;
+  VCK(cudaMemcpyAsync(c->d_raw, static_cast<const uint8_t*>(raw_host) + first, bytes, cudaMemcpyHostToDevice, s));
+  if (first == 0) {
+    VCK(cudaMemcpyAsync(c->d_raw_offsets32, offsets_host, 4ull * (n + 1), cudaMemcpyHostToDevice, s));
+  } else {
+    std::vector<uint32_t> rebased(offsets_host, offsets_host + n + 1);
+    for (auto& v : rebased) v -= first;
+    VCK(cudaMemcpyAsync(c->d_raw_offsets32, rebased.data(), 4ull * (n + 1), cudaMemcpyHostToDevice, s));
+    VCK(cudaStreamSynchronize(s));
+  }
+  return 0;
+}
+
+int velo_run_host_u32(VeloCtx* c, const void* raw_host, const uint32_t* raw_offsets_host, uint32_t n_events,
+                      void* stream, VeloOutputs* out)
+{
+  if (!c || !raw_host || !raw_offsets_host) return VELO_ERR_INVALID;
+  if (n_events > c->cfg.max_events) return VELO_ERR_CAPACITY;
+  if (static_cast<uint64_t>(raw_offsets_host[n_events]) - raw_offsets_host[0] > c->cfg.max_raw_bytes)
+    return VELO_ERR_CAPACITY;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (cudaSetDevice(c->device) != cudaSuccess) return VELO_ERR_CUDA;
+  const int rc = upload_batch_u32(c, raw_host, raw_offsets_host, n_events, s);
+  if (rc) return rc;
+  return velo_run_u32(c, c->d_raw, c->d_raw_offsets32, n_events, stream, out);
 }
 
 int velo_run_host(VeloCtx* c, const void* raw_host, const uint64_t* raw_offsets_host, uint32_t n_events, void* stream,
@@ -718,9 +899,27 @@ int velo_set_mlp(VeloCtx* c, const void* weights_host, size_t bytes)
   return 0;
 }
 
+int velo_capture_labels(VeloCtx* c, int ext, uint32_t max_event_clusters)
+{
+  if (!c) return VELO_ERR_INVALID;
+  if (c->mode != VELO_MODE_PLAIN || c->last_n == 0) return VELO_ERR_STATE;
+  if (cudaSetDevice(c->device) != cudaSuccess) return VELO_ERR_CUDA;
+  if (!c->d_labels) VCK(dalloc(c->d_labels, c->hit_capacity));
+  drop_graphs(c);  // the launch parameters of the label mode change
+  const ChainPointers P = pointers(c, c->last_n);
+  capture_labels_kernel<<<std::min<uint32_t>(c->last_n, 8u * c->sm_count), 256, 0, c->last_stream>>>(
+    P, c->d_labels, max_event_clusters);
+  VCK(cudaGetLastError());
+  VCK(cudaStreamSynchronize(c->last_stream));
+  c->labels_ready = true;
+  c->labels_ext = ext ? 1u : 0u;
+  c->labels_max_hits = max_event_clusters;
+  return 0;
+}
+
 int velo_set_mode(VeloCtx* c, uint32_t mode)
 {
-  if (!c || (mode != VELO_MODE_PLAIN && mode != VELO_MODE_PRUNED)) return VELO_ERR_INVALID;
+  if (!c || (mode != VELO_MODE_PLAIN && mode != VELO_MODE_PRUNED && mode != VELO_MODE_LABELS)) return VELO_ERR_INVALID;
   if (mode != c->mode) drop_graphs(c);
   c->mode = mode;
   return 0;
@@ -738,7 +937,13 @@ int velo_set_timing(VeloCtx* c, int enabled)
 {
   if (!c) return VELO_ERR_INVALID;
   if (cudaSetDevice(c->device) != cudaSuccess) return VELO_ERR_CUDA;
-  while (c->ev_sets.size() < kPlainEventSets) {
+  if (enabled && !c->timing) {
+    // graphs captured without the stage events are captured again, with them
+    bool untimed = false;
+    for (auto& kv : c->graphs) untimed |= !kv.second.timed;
+    if (untimed) drop_graphs(c);
+  }
+  while (c->ev_sets.size() < kEventSets) {
     const int rc = add_event_set(c);
     if (rc < 0) return rc;
   }
@@ -820,6 +1025,13 @@ int velo_check_wait_timeout(VeloCtx* c, uint32_t polls, void* stream)
   return 0;
 }
 
+int velo_graph_count(VeloCtx* c, uint32_t* n)
+{
+  if (!c || !n) return VELO_ERR_INVALID;
+  *n = static_cast<uint32_t>(c->graphs.size());
+  return 0;
+}
+
 int velo_last_launch_count(VeloCtx* c, uint32_t* n)
 {
   if (!c || !n) return VELO_ERR_INVALID;
@@ -842,7 +1054,7 @@ int velo_destroy(VeloCtx* c)
 bool velo_ctx_last_run(VeloCtx* c, ChainPointers* P, cudaStream_t* stream, int* device)
 {
   if (!c || !P || c->last_n == 0) return false;
-  *P = pointers(c, nullptr, nullptr, c->last_n);
+  *P = pointers(c, c->last_n);
   *stream = c->last_stream;
   *device = c->device;
   return true;

@@ -11,7 +11,7 @@ namespace velo {
 __global__ void __launch_bounds__(1024) event_scan_kernel(ChainPointers P)
 {
   __shared__ uint32_t s_warp_t[32], s_warp_h[32];
-  const uint32_t N = P.n_events;
+  const uint32_t N = P.run->n_events;
   const uint32_t per = (N + blockDim.x - 1) / blockDim.x;
   const uint32_t a = min(N, threadIdx.x * per), b = min(N, a + per);
   uint32_t t = 0, h = 0;
@@ -259,8 +259,8 @@ __global__ void __launch_bounds__(WPB * 32) consolidate_fit_kernel(ChainPointers
   __shared__ float s_hit[WPB][3][kConsolidateStage];
   const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
   const uint32_t e = blockIdx.x * WPB + warp;
-  if (e >= P.n_events) return;
-  const uint32_t N = P.n_events;
+  const uint32_t N = P.run->n_events;
+  if (e >= N) return;
   const uint32_t T = P.atomics[2 * N];
   const uint32_t Htot = P.event_hit_offset[N];
   const uint32_t nt = P.atomics[e];

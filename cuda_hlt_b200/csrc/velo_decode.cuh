@@ -36,7 +36,11 @@ __device__ __forceinline__ void window_add(SpWindow& w, uint32_t o, int32_t r, i
   const uint32_t osp = sp_mask(o);
   if (!sp_isolated(o) && orow >= r - 2 && orow <= r + 1 && ocol >= c - 1 && ocol <= c + 1) {
     const int32_t rr = orow - (r - 2), rc = ocol - (c - 1);
-    w.px[rc] |= (osp & 0x0Fu) << (4 * rr) | (osp & 0xF0u) << (12 + 4 * rr);
+    const uint32_t v = (osp & 0x0Fu) << (4 * rr) | (osp & 0xF0u) << (12 + 4 * rr);
+    // constant register indices: a runtime index would put the window in local memory
+    w.px[0] |= rc == 0 ? v : 0u;
+    w.px[1] |= rc == 1 ? v : 0u;
+    w.px[2] |= rc == 2 ? v : 0u;
   }
   if (ocol == c) {
     if (orow == r + 1) w.top |= osp;
@@ -171,6 +175,9 @@ struct DecodeShared {
   uint32_t mod_count[kModules];  // clusters per module
   uint32_t mod_start[kModules];  // exclusive scan of mod_count: compact layout
   uint32_t event;
+  uint32_t n_events;             // events of the run
+  uint32_t skipped;              // 1: position left empty (beyond the selection); 2: bad list entry
+  uint64_t ev_off, ev_bytes;     // the event's raw bytes: offset in the batch and size
   uint32_t flags;
   uint32_t n_candidates;
   uint32_t n_list;
@@ -316,8 +323,62 @@ __device__ __forceinline__ void warp_smem_sort(unsigned long long* key, uint32_t
   }
 }
 
-// 40 warps per SM (5 blocks of 8): 48 registers, no spills
-template<int W>
+// Shared-memory capacity for the event's phi in the windows pass (the union below, free once
+// the modules are sorted); larger events search their windows in the cluster records.
+constexpr uint32_t kPhiStageCap = (kCandCap * 4 + kBankMapCap + kNonIsoCap * 2) / 4;
+
+// Phi windows of the h1 of one module, after the event's modules are sorted
+// (fill_candidates, FillCandidates.cu:8-70, VeloTools.cuh:6-42): for each hit h1 of module m
+// (2..49) the hits within kPhiExtrapolation of phi(h1) in module m + 2 (h0) and m - 2 (h2),
+// as event-relative u16 pairs {first | last << 16} (0xFFFF: none). `sphi` holds the event's
+// phi in hit order (null: read the cluster records). In the pruned mode also the scorer's
+// inputs: keep bits (3: seeding candidate, verdict to come; 2: no seed) and, for each
+// candidate the gates admit, an 8-byte record (event hit base, h1 | m << 16) appended to the
+// candidate list (queue slot 7). One warp per module; every lane takes part in each 32-hit
+// round (ballots).
+template<bool kPruned>
+__device__ __forceinline__ void module_windows(const ChainPointers& P, const float* sphi, const float4* H, uint2* Wn,
+                                               uint8_t* K, uint32_t base, uint32_t m, const uint32_t* mstart,
+                                               const uint32_t* mcount, bool score)
+{
+  const uint32_t lane = lane_id();
+  const uint32_t s1 = mstart[m], n1 = mcount[m];
+  const uint32_t s0 = mstart[m + 2], n0 = mcount[m + 2], s2 = mstart[m - 2], n2 = mcount[m - 2];
+  for (uint32_t r0 = 0; r0 < n1; r0 += 32) {
+    const uint32_t r = r0 + lane;
+    const bool valid = r < n1;
+    const uint32_t h = s1 + r;
+    int f0 = -1, l0 = -1, f2 = -1, l2 = -1;
+    if (valid) {
+      if (sphi) {
+        const float p = sphi[h];
+        if (n0 > 0) phi_window(sphi, s0, n0, p, kPhiExtrapolation, f0, l0);
+        if (n2 > 0) phi_window(sphi, s2, n2, p, kPhiExtrapolation, f2, l2);
+      } else {
+        const float p = H[h].w;
+        if (n0 > 0) phi_window4(H, s0, n0, p, kPhiExtrapolation, f0, l0);
+        if (n2 > 0) phi_window4(H, s2, n2, p, kPhiExtrapolation, f2, l2);
+      }
+      Wn[h] = make_uint2((static_cast<uint32_t>(f0) & 0xFFFFu) | (static_cast<uint32_t>(l0) << 16),
+                         (static_cast<uint32_t>(f2) & 0xFFFFu) | (static_cast<uint32_t>(l2) << 16));
+    }
+    if (kPruned) {
+      const bool cand = valid && f0 != -1 && f2 != -1;
+      if (valid) K[h] = cand ? 3u : 2u;  // candidates: verdict from score_candidates
+      // seeds whose pair loop is cheaper than their scoring stay kept, unscored
+      const bool append = cand && score && static_cast<uint32_t>((l0 - f0) * (l2 - f2)) >= P.mlp.min_pairs;
+      const uint32_t bal = __ballot_sync(0xFFFFFFFFu, append);
+      uint32_t row0 = 0;
+      if (lane == 0 && bal) row0 = atomicAdd(P.queue + 7, static_cast<uint32_t>(__popc(bal)));
+      row0 = __shfl_sync(0xFFFFFFFFu, row0, 0);
+      if (append) P.cand_rec[row0 + __popc(bal & ((1u << lane) - 1u))] = make_uint2(base, h | (m << 16));
+    }
+  }
+}
+
+// 40 warps per SM (5 blocks of 8): 48 registers, no spills. kPruned: the windows pass also
+// prepares the learned scorer's candidate list.
+template<int W, bool kPruned>
 __global__ void __launch_bounds__(W * 32, 40 / W) decode_cluster_sort_kernel(ChainPointers P)
 {
   __shared__ DecodeShared sh;
@@ -335,7 +396,25 @@ __global__ void __launch_bounds__(W * 32, 40 / W) decode_cluster_sort_kernel(Cha
 
   for (;;) {
     if (threadIdx.x == 0) {
-      sh.event = atomicAdd(P.queue + 0, 1u);
+      // the event of this pass and its raw bytes, for the whole block
+      const uint32_t e = atomicAdd(P.queue + 0, 1u);
+      const RunParams& R = *P.run;
+      sh.event = e;
+      sh.n_events = R.n_events;
+      if (e < R.n_events) {
+        uint32_t src = e;  // raw event of this position
+        uint32_t skipped = 0;
+        if (P.event_list) {  // the global event cut of this chain
+          if (e < *P.n_selected) src = P.event_list[e];
+          else skipped = 1;
+        } else if (R.event_list) {  // a selection made by the caller
+          src = R.event_list[e];
+          if (src >= R.n_raw) skipped = 2;
+        }
+        sh.skipped = skipped;
+        sh.ev_off = skipped ? 0 : raw_offset(R, src);
+        sh.ev_bytes = skipped ? 0 : raw_offset(R, src + 1) - sh.ev_off;
+      }
       sh.flags = 0;
       sh.n_candidates = 0;
       sh.n_list = 0;
@@ -345,16 +424,11 @@ __global__ void __launch_bounds__(W * 32, 40 / W) decode_cluster_sort_kernel(Cha
     if (threadIdx.x < kModules) sh.mod_count[threadIdx.x] = 0;
     __syncthreads();
     const uint32_t e = sh.event;
-    if (e >= P.n_events) break;
-    uint32_t src = e;  // raw event of this position
-    bool skipped = false;
-    if (P.event_list) {
-      if (e < *P.n_selected) src = P.event_list[e];
-      else skipped = true;
-    }
-    const uint64_t off = skipped ? 0 : P.raw_offsets[src];
-    const uint64_t bytes = skipped ? 0 : P.raw_offsets[src + 1] - off;
-    const uint32_t* ev = reinterpret_cast<const uint32_t*>(P.raw + off);
+    if (e >= sh.n_events) break;
+    const uint32_t skipped = sh.skipped;
+    const uint64_t off = sh.ev_off;
+    const uint64_t bytes = sh.ev_bytes;
+    const uint32_t* ev = reinterpret_cast<const uint32_t*>(P.run->raw + off);
     const uint64_t words = bytes / 4;
     const uint32_t header = 2 + kSensors;  // number_of_raw_banks + raw_bank_offset[209]
     // ---- validate the raw event and index its banks ----
@@ -382,7 +456,7 @@ __global__ void __launch_bounds__(W * 32, 40 / W) decode_cluster_sort_kernel(Cha
         if (count > 256) atomicOr(&sh.flags, kStatusBigSpIndex);
       }
     } else if (threadIdx.x == 0) {
-      atomicOr(&sh.flags, skipped ? kStatusNotSelected : kStatusBadRawEvent);
+      atomicOr(&sh.flags, skipped == 1 ? kStatusNotSelected : kStatusBadRawEvent);
     }
     __syncthreads();
     const bool event_ok = !(sh.flags & (kStatusBadRawEvent | kStatusNotSelected));
@@ -572,6 +646,32 @@ __global__ void __launch_bounds__(W * 32, 40 / W) decode_cluster_sort_kernel(Cha
       if (lane == 0) {
         P.module_start[e * kModules + m] = p0;
         P.module_num[e * kModules + m] = n;
+      }
+    }
+    __syncthreads();
+    // ---- phi windows of every h1 (fill_candidates), while the event is in L2: the sorted phi
+    // are read back into the shared memory the lists and sort buffers no longer need ----
+    {
+      const uint32_t nh = write ? sh.mod_start[kModules - 1] + sh.mod_count[kModules - 1] : 0;
+      if (nh > 0 && nh <= kEventHitCap) {  // the events the search runs
+        const float4* H = P.hits.xyzp + base;
+        float* sphi = nh <= kPhiStageCap ? reinterpret_cast<float*>(&su) : nullptr;
+        if (sphi)
+          for (uint32_t i = threadIdx.x; i < nh; i += blockDim.x) sphi[i] = H[i].w;
+        __syncthreads();
+        bool score = false;
+        uint8_t* K = nullptr;
+        if (kPruned) {
+          K = P.keep + base;
+          const bool fallback = nh > P.mlp.max_hits;  // above the trained occupancy: plain search
+          if (fallback && threadIdx.x == 0) sh.flags |= kStatusMlpFallback;
+          score = !fallback && nh >= P.mlp.min_hits;
+          // modules 0, 1, 50, 51 hold no h1: extension candidates only
+          for (uint32_t h = threadIdx.x; h < sh.mod_start[2]; h += blockDim.x) K[h] = 2;
+          for (uint32_t h = sh.mod_start[50] + threadIdx.x; h < nh; h += blockDim.x) K[h] = 2;
+        }
+        for (uint32_t m = 2 + warp; m < 50; m += W)
+          module_windows<kPruned>(P, sphi, H, P.windows + base, K, base, m, sh.mod_start, sh.mod_count, score);
       }
     }
     __syncthreads();

@@ -1,14 +1,8 @@
-// Kernel 2 of the chain: fill_candidates. For every hit h1 of modules 2..49 the phi windows
-// of h0 (module m+2) and h2 (module m-2) with the reference's searches and tolerance
-// (FillCandidates.cu:8-70, VeloTools.cuh:6-42). The reference computes them in a kernel of
-// their own too; here one thread per hit (a 256-thread CTA per event, persistent, queue slot
-// 3) writes them as event-relative u16 pairs {first, last} (0xFFFF = none), so the search
-// kernel reads a window instead of binary-searching inside its serial module loop.
-//
-// Pruned mode, three kernels:
-//   fill_candidates<true>  also appends every seeding candidate (both windows non-empty)
-//                          that the scoring gate admits to a compact list, as an 8-byte
-//                          record (event hit base, h1, module; queue slot 7 counts them);
+// The learned scorer's kernels between decode and search (pruned mode). The decode kernel
+// computes the phi windows of every h1 (fill_candidates, FillCandidates.cu:8-70) and, in the
+// pruned mode, appends every seeding candidate (both windows non-empty) that the scoring gate
+// admits to a compact list as an 8-byte record (event hit base, h1, module; queue slot 7
+// counts them). Then:
 //   candidate_features     a thread per listed candidate (all lanes busy, full occupancy)
 //                          computes its twelve proxy-triplet features and writes them,
 //                          normalised and in bf16, as a row of 128-row tiles laid out for
@@ -30,82 +24,6 @@ namespace velo {
 constexpr uint32_t kErrorMlpTimeout = 1u;  // queue[6]: the tensor core did not answer in time
 constexpr uint32_t kFillThreads = 256;
 constexpr uint32_t kCandTileBytes = kMlpTile * kMlpK1 * 2;  // 4096
-
-__device__ __forceinline__ uint2 pack_windows(int f0, int l0, int f2, int l2)
-{
-  return make_uint2((static_cast<uint32_t>(f0) & 0xFFFFu) | (static_cast<uint32_t>(l0) << 16),
-                    (static_cast<uint32_t>(f2) & 0xFFFFu) | (static_cast<uint32_t>(l2) << 16));
-}
-
-template<bool kPruned>
-__global__ void __launch_bounds__(kFillThreads) fill_candidates_kernel(ChainPointers P)
-{
-  __shared__ uint32_t s_ms[kModules + 1];
-  __shared__ uint32_t s_event;
-  const uint32_t lane = threadIdx.x & 31u;
-
-  for (;;) {
-    if (threadIdx.x == 0) s_event = atomicAdd(P.queue + 3, 1u);
-    __syncthreads();
-    const uint32_t e = s_event;
-    if (e >= P.n_events) break;
-    const uint32_t nhits = P.event_hits[e];
-    const uint32_t base = P.event_hit_base[e];
-    const uint32_t status = P.status[e];
-    const bool runnable = !(status & (kStatusBadRawEvent | kStatusHitOverflow)) && nhits <= kEventHitCap && nhits > 0;
-    if (threadIdx.x < kModules) s_ms[threadIdx.x] = P.module_start[e * kModules + threadIdx.x] - base;
-    if (threadIdx.x == 0) s_ms[kModules] = nhits;
-    __syncthreads();
-    if (runnable) {
-      const float4* H = P.hits.xyzp + base;
-      uint2* W = P.windows + base;
-      const bool fallback = kPruned && nhits > P.mlp.max_hits;
-      if (kPruned && fallback && threadIdx.x == 0) P.status[e] = status | kStatusMlpFallback;
-      const uint32_t lo = s_ms[2], hi = s_ms[50];
-      if (kPruned) {
-        // modules 0, 1, 50, 51 hold no h1: extension candidates only
-        uint8_t* K = P.keep + base;
-        for (uint32_t h = threadIdx.x; h < lo; h += kFillThreads) K[h] = 2;
-        for (uint32_t h = hi + threadIdx.x; h < nhits; h += kFillThreads) K[h] = 2;
-      }
-      for (uint32_t t0 = lo; t0 < hi; t0 += kFillThreads) {
-        const uint32_t h = t0 + threadIdx.x;
-        const bool valid = h < hi;
-        int f0 = -1, l0 = -1, f2 = -1, l2 = -1;
-        uint32_t m = 2;
-        if (valid) {
-          uint32_t a = 2, b = 50;  // last module with start <= h
-          while (b - a > 1) {
-            const uint32_t mid = (a + b) >> 1;
-            if (s_ms[mid] <= h) a = mid; else b = mid;
-          }
-          m = a;
-          const float p = H[h].w;
-          const uint32_t n0 = s_ms[m + 3] - s_ms[m + 2], n2 = s_ms[m - 1] - s_ms[m - 2];
-          if (n0 > 0) phi_window4(H, s_ms[m + 2], n0, p, kPhiExtrapolation, f0, l0);
-          if (n2 > 0) phi_window4(H, s_ms[m - 2], n2, p, kPhiExtrapolation, f2, l2);
-          W[h] = pack_windows(f0, l0, f2, l2);
-        }
-        if (kPruned) {
-          const bool cand = valid && f0 != -1 && f2 != -1;
-          if (valid) P.keep[base + h] = cand ? 3u : 2u;  // candidates: verdict from score_candidates
-          // seeds whose pair loop is cheaper than their scoring stay kept, unscored
-          const bool append = cand && !fallback && nhits >= P.mlp.min_hits &&
-                              static_cast<uint32_t>((l0 - f0) * (l2 - f2)) >= P.mlp.min_pairs;
-          // one atomic per warp for the rows of its candidates; the features follow in
-          // candidate_features, densely
-          const uint32_t bal = __ballot_sync(0xFFFFFFFFu, append);
-          uint32_t row0 = 0;
-          if (lane == 0 && bal) row0 = atomicAdd(P.queue + 7, static_cast<uint32_t>(__popc(bal)));
-          row0 = __shfl_sync(0xFFFFFFFFu, row0, 0);
-          if (append) P.cand_rec[row0 + __popc(bal & ((1u << lane) - 1u))] = make_uint2(base, h | (m << 16));
-        }
-      }
-    }
-    __syncthreads();
-  }
-}
-
 
 // Features of the listed candidates: a thread per row, grid-stride over queue slot 7's rows.
 __global__ void __launch_bounds__(kFillThreads) candidate_features_kernel(ChainPointers P)

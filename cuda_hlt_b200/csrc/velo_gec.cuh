@@ -27,12 +27,7 @@ constexpr uint32_t kGecThreads = 256;
 constexpr uint32_t kGecListThreads = 1024;
 
 struct GecPointers {
-  const uint8_t* ut_raw;
-  const uint64_t* ut_offsets;     // [N+1] byte offsets
-  const uint8_t* scifi_raw;
-  const uint64_t* scifi_offsets;  // [N+1]
-  uint32_t n_events;
-  uint32_t max_clusters;
+  const RunParams* run;  // inputs: UT and SciFi raw events, their offsets, the threshold
   uint32_t* counts;      // [2N] {SciFi estimate, UT hits} per event (0xFFFFFFFF when malformed)
   uint8_t* flags;        // [N] kGecPass | kGecMalformed
   uint32_t* event_list;  // [N] passing events, ascending
@@ -56,12 +51,13 @@ __global__ void __launch_bounds__(kGecThreads) gec_count_kernel(GecPointers G)
 {
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t warps = gridDim.x * (kGecThreads / 32);
-  for (uint32_t e = blockIdx.x * (kGecThreads / 32) + (threadIdx.x >> 5); e < G.n_events; e += warps) {
+  const RunParams& R = *G.run;
+  for (uint32_t e = blockIdx.x * (kGecThreads / 32) + (threadIdx.x >> 5); e < R.n_events; e += warps) {
     // SciFi: only the bank offset table is read
     const uint32_t* sf;
     uint32_t nb = 0;
     uint64_t bytes = 0;
-    bool bad = !gec_table(G.scifi_raw, G.scifi_offsets, e, sf, nb, bytes);
+    bool bad = !gec_table(R.scifi_raw, R.scifi_offsets, e, sf, nb, bytes);
     uint32_t sum = 0;
     if (!bad)
       for (uint32_t i = lane; i < nb; i += 32)
@@ -71,7 +67,7 @@ __global__ void __launch_bounds__(kGecThreads) gec_count_kernel(GecPointers G)
     // UT: the hit count in each bank's second word
     const uint32_t* ut;
     uint32_t nu = 0;
-    bool ut_bad = !gec_table(G.ut_raw, G.ut_offsets, e, ut, nu, bytes);
+    bool ut_bad = !gec_table(R.ut_raw, R.ut_offsets, e, ut, nu, bytes);
     uint64_t hits = 0;
     if (!ut_bad) {
       const uint64_t payload = bytes - (static_cast<uint64_t>(nu) + 2) * 4;
@@ -91,8 +87,8 @@ __global__ void __launch_bounds__(kGecThreads) gec_count_kernel(GecPointers G)
     }
     if (lane == 0) {
       const uint32_t n_ut = ut_bad ? 0xFFFFFFFFu : static_cast<uint32_t>(hits < 0xFFFFFFFEull ? hits : 0xFFFFFFFEull);
-      const bool pass = !bad && !ut_bad && n_scifi < G.max_clusters &&
-                        hits + static_cast<uint64_t>(n_scifi) < G.max_clusters;
+      const bool pass = !bad && !ut_bad && n_scifi < R.gec_max &&
+                        hits + static_cast<uint64_t>(n_scifi) < R.gec_max;
       G.counts[2 * e] = bad ? 0xFFFFFFFFu : n_scifi;
       G.counts[2 * e + 1] = n_ut;
       G.flags[e] = (pass ? kGecPass : 0) | (bad || ut_bad ? kGecMalformed : 0);
@@ -105,8 +101,9 @@ __global__ void __launch_bounds__(kGecListThreads) gec_list_kernel(GecPointers G
 {
   __shared__ uint32_t s_warp[kGecListThreads / 32];
   const uint32_t t = threadIdx.x, lane = t & 31u;
-  const uint32_t per = (G.n_events + kGecListThreads - 1) / kGecListThreads;
-  const uint32_t begin = min(t * per, G.n_events), end = min(begin + per, G.n_events);
+  const uint32_t n_events = G.run->n_events;
+  const uint32_t per = (n_events + kGecListThreads - 1) / kGecListThreads;
+  const uint32_t begin = min(t * per, n_events), end = min(begin + per, n_events);
   uint32_t mine = 0;
   for (uint32_t e = begin; e < end; ++e) mine += G.flags[e] & kGecPass;
   uint32_t incl = mine;

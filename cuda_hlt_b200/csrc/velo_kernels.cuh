@@ -73,11 +73,35 @@ struct SearchScratch {
   uint16_t* weak;          // [N * kWeakCap * 3]
 };
 
-struct ChainPointers {
-  // input
+// Inputs of one run, read by the kernels from device memory: set_run_kernel writes them
+// before each run, so that a CUDA graph captured for a batch-size bucket serves every batch
+// of that bucket, wherever its buffers are.
+struct RunParams {
   const uint8_t* raw;
-  const uint64_t* raw_offsets;  // [N+1]
+  const uint64_t* raw_offsets;    // [n_events + 1] byte offsets, or null: raw_offsets32
+  const uint32_t* raw_offsets32;  // [n_events + 1] u32 byte offsets (the reference's own format)
   uint32_t n_events;
+  const uint32_t* event_list;     // [n_events] raw event decoded at each position, or null
+                                  // (identity); entries at or beyond n_raw mark the position bad
+  uint32_t n_raw;                 // raw events in the batch (with event_list)
+  uint32_t gec_max;               // global event cut threshold (velo_run_gec)
+  const uint8_t* ut_raw;          // global event cut inputs (null without the cut)
+  const uint64_t* ut_offsets;
+  const uint8_t* scifi_raw;
+  const uint64_t* scifi_offsets;
+};
+
+__device__ __forceinline__ uint64_t raw_offset(const RunParams& R, uint32_t e)
+{
+  return R.raw_offsets ? R.raw_offsets[e] : static_cast<uint64_t>(R.raw_offsets32[e]);
+}
+
+struct ChainPointers {
+  // input: the run's parameters in device memory; n_grid is the number of events the launch
+  // grids are sized for (the bucket of a graph, at least run->n_events): kernels take the
+  // run's own count from run->n_events
+  const RunParams* run;
+  uint32_t n_grid;
   // global event cut (null without it): position e < *n_selected decodes raw event
   // event_list[e]; later positions are left empty
   const uint32_t* event_list;

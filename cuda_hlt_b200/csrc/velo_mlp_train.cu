@@ -757,7 +757,7 @@ int velo_mlp_collect(VeloMlpTrainer* t, VeloCtx* ctx, uint64_t* n_total)
   if (dev != t->device) return VELO_ERR_INVALID;
   if (P.keep) return VELO_ERR_STATE;  // labels come from the plain search only
   if (cudaSetDevice(t->device) != cudaSuccess) return VELO_ERR_CUDA;
-  const uint32_t N = P.n_events;
+  const uint32_t N = P.n_grid;  // the last run's events (its kernels were sized for them)
   if (N == 0 || t->n >= t->cap) {
     if (n_total) *n_total = t->n;
     return 0;

@@ -118,9 +118,9 @@ __global__ void __launch_bounds__(kPvThreads) pv_beamline_kernel(ChainPointers P
 {
   __shared__ PvSmem s;
   const uint32_t e = blockIdx.x;
-  if (e >= P.n_events) return;
+  const uint32_t N = P.run->n_events;
+  if (e >= N) return;
   const uint32_t warp = threadIdx.x >> 5, lane = lane_id();
-  const uint32_t N = P.n_events;
   const uint32_t T = P.atomics[2 * N];
   const uint32_t nt = P.atomics[e];
   const uint32_t t0 = P.atomics[N + e];

@@ -1,5 +1,6 @@
-"""Small fixed workload for profiler captures: one batch of nu ~ U(2,15) events, run
-`--runs` times through the chain (device-resident input, no graphs).
+"""Small fixed workload for profiler captures: one batch of events of a synthetic workload
+(default nu ~ U(2,15)), run `--runs` times through the chain (device-resident input, no
+graphs, default output capacities: 400 tracks per event).
 
 python -m cuda_hlt_b200.profile_case [--events 8192] [--runs 2] [--block-threshold N] [--mode plain|pruned] [--pv]
                                      [--gec]
@@ -34,8 +35,7 @@ def main():
         ut, sf = events.generate_ut_scifi(b, seed=0)
         gec = [torch.from_numpy(a).cuda() for a in (ut.raw, ut.offsets.view(np.int64), sf.raw,
                                                      sf.offsets.view(np.int64))]
-    vc = chain.VeloChain(max_events=args.events, max_raw_bytes=int(b.raw.size) + 4096, max_tracks=160 * args.events,
-                         max_track_hits=12 * 160 * args.events)
+    vc = chain.VeloChain(max_events=args.events, max_raw_bytes=int(b.raw.size) + 4096)
     vc.set_block_threshold(args.block_threshold)
     vc.set_pv(args.pv)
     if args.mode == "pruned":

@@ -153,6 +153,9 @@ typedef struct VeloCtx VeloCtx;
 
 #define VELO_MODE_PLAIN 0  /* exhaustive search_by_triplet (reference semantics) */
 #define VELO_MODE_PRUNED 1 /* learned seed/extension scorer prunes the search */
+#define VELO_MODE_LABELS 2 /* pruned by the plain search's own labels of the same batch
+                              (velo_capture_labels): a perfect scorer at no cost, which measures
+                              how much pruning can save at most */
 
 /* Search mapping (velo_set_block_threshold sets the boundary directly). */
 #define VELO_MAP_AUTO 0    /* search: block per event above 1,536 clusters, warp per event below */
@@ -167,7 +170,12 @@ typedef struct VeloConfig {
   int32_t device;               /* CUDA device ordinal */
   uint32_t mode;                /* VELO_MODE_* */
   uint32_t mapping;             /* VELO_MAP_* */
-  uint32_t use_graphs;          /* capture the launch sequence in CUDA graphs per bucket */
+  uint32_t use_graphs;          /* capture the launch sequence in CUDA graphs, one per batch-size
+                                   bucket (1,024 events x a power of 4, at most max_events), stream
+                                   and global event cut on/off; the kernels read each run's inputs
+                                   from a device-side parameter block, so a graph serves every
+                                   batch of its bucket wherever its buffers are; at most 16 graphs
+                                   are kept, the least recently launched evicted first */
 } VeloConfig;
 
 /* Output buffers of one velo_run call: device pointers, valid until the next velo_run on
@@ -210,6 +218,11 @@ typedef struct VeloOutputs {
   uint32_t* gec_counts;  /* [2 * n_events] per raw event: SciFi cluster estimate, UT hits
                             (0xFFFFFFFF: malformed bank table) */
   uint8_t* gec_flags;    /* [n_events] per raw event: VELO_GEC_PASS | VELO_GEC_MALFORMED */
+  /* fill_candidates output (dev_h0_candidates / dev_h2_candidates of FillCandidates.cu:72):
+   * per hit of modules 2..49, indexed like hit_xyzp, two u32 {first | last << 16} of its h0
+   * window (module + 2) and h2 window (module - 2), event-relative, 0xFFFF: none; in
+   * VELO_MODE_PRUNED a pruned seed has no h0 window */
+  uint32_t* hit_windows;
 } VeloOutputs;
 
 /* A primary vertex, in the layout of PV::Vertex (cuda/PV/beamlinePV/include/PV_Definitions.cuh:64-109). */
@@ -236,6 +249,22 @@ int velo_run(VeloCtx* ctx, const void* raw, const uint64_t* raw_offsets, uint32_
  * buffers on the stream, then runs. */
 int velo_run_host(VeloCtx* ctx, const void* raw_host, const uint64_t* raw_offsets_host, uint32_t n_events,
                   void* stream, VeloOutputs* out);
+
+/* velo_run and velo_run_host with u32 byte offsets, the reference's own input format
+ * (RuntimeOptions::host_velopix_offsets, main/include/RuntimeOptions.h:9-55, filled by
+ * main/src/InputReader.cpp:28-57): no widening pass on the caller's side. */
+int velo_run_u32(VeloCtx* ctx, const void* raw, const uint32_t* raw_offsets, uint32_t n_events, void* stream,
+                 VeloOutputs* out);
+int velo_run_host_u32(VeloCtx* ctx, const void* raw_host, const uint32_t* raw_offsets_host, uint32_t n_events,
+                      void* stream, VeloOutputs* out);
+
+/* The chain on a selection of the batch's n_raw events (device inputs, u32 offsets[n_raw + 1]):
+ * position e (< n_events) decodes raw event event_list[e] (device array), as the reference's
+ * VELO kernels read dev_event_list after global_event_cut_t (EstimateInputSize.cu:14-19 and
+ * the other kernels of the sequence). An entry at or beyond n_raw leaves its position empty
+ * with VELO_STATUS_BAD_RAW. */
+int velo_run_selected_u32(VeloCtx* ctx, const void* raw, const uint32_t* raw_offsets, uint32_t n_raw,
+                          const uint32_t* event_list, uint32_t n_events, void* stream, VeloOutputs* out);
 
 /* Global event cut in front of the chain: global_event_cut_t
  * (cuda/global_event_cut/src/GlobalEventCut.cu:3-55, configuration/sequences/Velo.h:7).
@@ -298,7 +327,17 @@ typedef struct VeloMlpWeights {
  * required before a run in VELO_MODE_PRUNED. */
 int velo_set_mlp(VeloCtx* ctx, const void* weights_host, size_t bytes);
 
-/* Switches the context between VELO_MODE_PLAIN and VELO_MODE_PRUNED. */
+/* Keeps, for every hit of the last run (plain mode, after velo_sync), the labels the scorer
+ * is trained on: bit 0 "on a final track", bit 1 "fourth or later hit of a final track".
+ * A following run in VELO_MODE_LABELS on the same batch (same raw events and offsets, so
+ * that the hits land in the same slots) seeds only from hits with bit 0 and, when ext is
+ * nonzero, forwards only onto hits with bit 1; events with more than max_event_clusters
+ * clusters are not pruned (VELO_STATUS_MLP_FALLBACK), as in VELO_MODE_PRUNED. Blocks until
+ * the labels are written. No counterpart in the reference: a measurement of the ceiling of
+ * learned pruning (the scorer's decisions replaced by the right answers, at no cost). */
+int velo_capture_labels(VeloCtx* ctx, int ext, uint32_t max_event_clusters);
+
+/* Switches the context between VELO_MODE_PLAIN, VELO_MODE_PRUNED and VELO_MODE_LABELS. */
 int velo_set_mode(VeloCtx* ctx, uint32_t mode);
 
 /* Trainer of the scorer on one device. Samples are the seeding candidates of plain runs,
@@ -365,6 +404,9 @@ int velo_check_wait_timeout(VeloCtx* ctx, uint32_t polls, void* stream);
 
 /* Kernel launch count of the last run (all kernels of this library). */
 int velo_last_launch_count(VeloCtx* ctx, uint32_t* n);
+
+/* CUDA graphs the context holds (VeloConfig.use_graphs). */
+int velo_graph_count(VeloCtx* ctx, uint32_t* n);
 
 /* Search without allocation, for callers that cannot allocate device memory (for example a
  * host framework that reserves the device up front and hands out fixed slices). No

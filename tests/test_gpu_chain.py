@@ -327,3 +327,110 @@ def test_bounded_wait_timeout_reported():
     t, _, c = vc.sync()
     assert t > 0 and c > 0
     vc.close()
+
+
+def _same_results(a, b, n_events, what):
+    """Equal outputs of two runs: dense outputs whole, clusters event by event (the cluster
+    buffers have unused gaps between events whose contents are not outputs)."""
+    for k in ("atomics", "track_hit_number", "hit_id", "hit_x", "status", "module_num"):
+        assert np.array_equal(a[k], b[k]), (what, k)
+    for e in range(n_events):
+        for ma, mb in zip(chain.event_clusters(a, e), chain.event_clusters(b, e)):
+            assert np.array_equal(ma["id"], mb["id"]) and np.array_equal(ma["phi"], mb["phi"]), (what, e)
+
+
+def test_u32_offsets_equal_u64():
+    """velo_run_host_u32 / velo_run_u32 take the reference's u32 offsets directly; results
+    equal the u64 entry points', also for a batch that starts inside the caller's buffer."""
+    import torch
+    b = events.generate_config("batched_500k", n_events=120, first_event=55)
+    ref = run_chain(b)
+    vc = chain.VeloChain(max_events=b.n_events, max_raw_bytes=int(b.raw.size) + 4096)
+    vc.run_host_u32(b.raw, b.offsets.astype(np.uint32))
+    vc.sync()
+    _same_results(ref, vc.results(), b.n_events, "host u32")
+    # events 20..119 of the same buffer: offsets rebased from a nonzero start
+    sub = b.subset(20, 120)
+    ref_sub = run_chain(sub)
+    vc.run_host_u32(b.raw, b.offsets[20:].astype(np.uint32))
+    vc.sync()
+    _same_results(ref_sub, vc.results(), sub.n_events, "host u32, rebased")
+    # device-resident input with u32 offsets
+    raw = torch.from_numpy(b.raw).cuda()
+    off = torch.from_numpy(b.offsets.astype(np.uint32).view(np.int32)).cuda()
+    vc.run_device_u32(raw.data_ptr(), off.data_ptr(), b.n_events, torch.cuda.current_stream().cuda_stream)
+    vc.sync()
+    _same_results(ref, vc.results(), b.n_events, "device u32")
+    vc.close()
+
+
+def test_selected_events_u32():
+    """velo_run_selected_u32 decodes the caller's selection (Allen's dev_event_list after
+    global_event_cut_t): position i holds raw event list[i], equal to a run over those events
+    alone; a list entry beyond the batch leaves its position empty and flagged."""
+    import torch
+    b = events.generate_config("batched_500k", n_events=64, first_event=300)
+    sel = np.array([3, 7, 8, 20, 41, 63, 0], np.uint32)
+    alone = events.EventBatch(np.concatenate([b.event(int(i)) for i in sel]),
+                              np.concatenate([[0], np.cumsum([b.event(int(i)).size for i in sel])]).astype(np.uint64))
+    ref = run_chain(alone)
+    raw = torch.from_numpy(b.raw).cuda()
+    off = torch.from_numpy(b.offsets.astype(np.uint32).view(np.int32)).cuda()
+    lst = torch.from_numpy(np.append(sel, 64).astype(np.uint32).view(np.int32)).cuda()
+    vc = chain.VeloChain(max_events=b.n_events, max_raw_bytes=int(b.raw.size) + 4096)
+    vc.n_events = len(sel) + 1
+    rc = vc.lib.velo_run_selected_u32(vc.ctx, chain.C.c_void_p(raw.data_ptr()), chain.C.c_void_p(off.data_ptr()),
+                                      b.n_events, chain.C.c_void_p(lst.data_ptr()), len(sel) + 1,
+                                      chain.C.c_void_p(torch.cuda.current_stream().cuda_stream), chain.C.byref(vc.out))
+    assert rc == 0
+    vc.sync()
+    got = vc.results()
+    vc.close()
+    n = len(sel)
+    assert got["status"][n] & chain.STATUS["bad_raw"] and got["n_tracks"][n] == 0
+    assert np.array_equal(got["status"][:n], ref["status"])
+    for e in range(n):
+        assert pu.canonical_tracks(chain.event_tracks(got, e)) == pu.canonical_tracks(chain.event_tracks(ref, e)), e
+        ids_a = np.concatenate([m["id"] for m in chain.event_clusters(got, e)])
+        ids_b = np.concatenate([m["id"] for m in chain.event_clusters(ref, e)])
+        assert np.array_equal(ids_a, ids_b), e
+
+
+def test_graph_per_bucket_serves_any_batch():
+    """With graphs, one graph per batch-size bucket (1,024 x 4^k events) serves batches of any
+    size in the bucket and in any buffers (the kernels read each run's inputs from a
+    device-side parameter block): results equal graph-free runs, the graph count is the
+    number of buckets used, every launch's stage times are recorded, and at most 16 graphs are
+    kept (least recently launched evicted)."""
+    import torch
+    sizes = (300, 1000, 1024, 1500, 700)
+    batches = [events.generate_config("batched_500k", n_events=n, first_event=1000 * i) for i, n in enumerate(sizes)]
+    refs = [run_chain(b) for b in batches]
+    cap = max(int(b.raw.size) for b in batches) + 4096
+    vc = chain.VeloChain(max_events=4096, max_raw_bytes=cap, use_graphs=True)
+    vc.set_timing(True)
+    s = torch.cuda.current_stream().cuda_stream
+    keep = []
+    for rep in range(2):
+        for b, ref in zip(batches, refs):
+            raw = torch.from_numpy(b.raw).cuda()  # a new buffer for every run
+            off = torch.from_numpy(b.offsets.view(np.int64)).cuda()
+            keep.append((raw, off))
+            vc.run_device(raw.data_ptr(), off.data_ptr(), b.n_events, s)
+            vc.sync()
+            _same_results(ref, vc.results(), b.n_events, (rep, b.n_events))
+    assert vc.graph_count() == 2  # buckets of 1,024 and 4,096 events
+    st = vc.stage_times()
+    assert st["runs"] == 2 * len(sizes) and st["search_by_triplet"] > 0
+    # one graph per stream: at most 16 kept
+    b = batches[0]
+    raw = torch.from_numpy(b.raw).cuda()
+    off = torch.from_numpy(b.offsets.view(np.int64)).cuda()
+    streams = [torch.cuda.Stream() for _ in range(20)]
+    for st_ in streams:
+        vc.run_device(raw.data_ptr(), off.data_ptr(), b.n_events, st_.cuda_stream)
+        st_.synchronize()
+    assert vc.graph_count() == 16
+    vc.sync()
+    _same_results(refs[0], vc.results(), batches[0].n_events, "after eviction")
+    vc.close()

@@ -265,3 +265,57 @@ def test_trained_scorer_prunes_at_no_efficiency_cost():
     _, st_plain = run_mode(big, chain.MODE_PLAIN, timing=True)
     _, st_pruned = run_mode(big, chain.MODE_PRUNED, w, timing=True)
     assert st_pruned["search_by_triplet"] < 0.95 * st_plain["search_by_triplet"]
+
+
+def test_label_mode_is_the_pruning_ceiling():
+    """VELO_MODE_LABELS prunes with the plain search's own labels of the same batch (a perfect
+    scorer at no cost). Every final track of the plain search - ghosts included - is made of
+    labelled hits, and a seed without the label only ever forms a tracklet that ends as a
+    rejected weak tracklet; the chosen extension of every final track is labelled. So label
+    pruning of seeds, and of extensions too, gives the plain tracks exactly, with less work:
+    the ceiling of what a scorer trained on these labels can save. With every event above the
+    occupancy limit nothing is pruned."""
+    b = events.generate(seed=14, nu_min=2.0, nu_max=20.0, n_events=512, with_mc=False)
+    vc = chain.VeloChain(max_events=b.n_events, max_raw_bytes=int(b.raw.size) + 4096)
+    with pytest.raises(chain.VeloError):  # no labels yet
+        vc.set_mode(chain.MODE_LABELS)
+        vc.run_host(b)
+    vc.set_mode(chain.MODE_PLAIN)
+    vc.run_host(b)
+    vc.sync()
+    plain = vc.results()
+    ref = canonical(plain, b.n_events)
+    defined = (plain["status"] & chain.REFERENCE_UNDEFINED) == 0
+    vc.capture_labels(ext=True, max_event_clusters=0)  # every event falls back
+    vc.set_mode(chain.MODE_LABELS)
+    vc.run_host(b)
+    vc.sync()
+    fb = vc.results()
+    assert canonical(fb, b.n_events) == ref
+    assert np.all((fb["status"] & chain.STATUS["mlp_fallback"]) != 0)
+    for ext in (False, True):
+        vc.set_mode(chain.MODE_PLAIN)
+        vc.run_host(b)
+        vc.sync()
+        vc.capture_labels(ext=ext)
+        vc.set_mode(chain.MODE_LABELS)
+        vc.run_host(b)
+        vc.sync()
+        lab = vc.results()
+        got = canonical(lab, b.n_events)
+        same = [got[e] == ref[e] for e in range(b.n_events)]
+        assert all(s for s, d in zip(same, defined) if d), (ext, [e for e in range(b.n_events) if not same[e]][:8])
+        assert defined.sum() >= 0.95 * b.n_events
+        assert not np.any(lab["status"] & chain.STATUS["mlp_fallback"])
+        # the labels as outputs: bit 0 exactly on the hits of the plain search's tracks, and
+        # seeds without it have no h0 window
+        ms, mn = lab["module_start"].reshape(-1, 52), lab["module_num"].reshape(-1, 52)
+        span = int((lab["module_start"] + lab["module_num"]).max())
+        win = vc._down(vc.out.hit_windows, np.uint32, 2 * span).reshape(-1, 2)
+        for e in range(0, b.n_events, 7):
+            a, z = int(ms[e, 0]), int(ms[e, 51] + mn[e, 51])
+            on_track = np.isin(lab["cluster_id"][a:z], [i for t in chain.event_tracks(plain, e) for i in t])
+            assert np.array_equal((lab["cluster_keep"][a:z] & 1).astype(bool), on_track), (ext, e)
+            lo, hi = int(ms[e, 2]), int(ms[e, 50])
+            assert np.all(win[lo:hi, 0][~on_track[lo - a:hi - a]] & 0xFFFF == 0xFFFF), (ext, e)
+    vc.close()
