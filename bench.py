@@ -145,7 +145,7 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
-TRAFFIC_SUMMARIES = ["velo_chain_pruned_1m_8192_ncu.md", "velo_chain_batched_8192_block1536_ncu.md"]
+TRAFFIC_SUMMARIES = ["velo_chain_pruned_1m_16384_ncu.md"]
 
 
 def load_traffic():
@@ -292,11 +292,15 @@ LABEL_FORMS = (("labels_seed", False, True), ("labels_seed_ext", True, True),
                ("labels_seed_ext_all_events", True, False))
 
 
-def run_quality(weights, n, threads):
-    """Long-track efficiency and ghost rate of both forms, and of the label-pruned forms,
-    against generator truth on the first n events of the workload (with MC truth)."""
+def run_quality(weights, n, threads, label_events=2 * SIDE_BATCH):
+    """Long-track efficiency and ghost rate of both forms against generator truth on the
+    first n events of the workload (with MC truth), and of the label-pruned forms on the first
+    label_events of them (their tracks equal the plain ones by construction; the GPU tests
+    check it event by event). Events above the scorer's trained occupancy run the plain search
+    in the pruned form; their number in the sample is reported."""
     rows = {"plain": [], "pruned": []}
     rows.update({name: [] for name, _, _ in LABEL_FORMS})
+    fallback = 0
 
     def add(name, b, res):
         c = chain.check_tracks(b, res)
@@ -312,23 +316,30 @@ def run_quality(weights, n, threads):
             vc.set_mode(mode)
             vc.run_host(b)
             vc.sync()
-            add(name, b, vc.results(clusters=False))
-        for name, ext, fallback in LABEL_FORMS:
-            vc.set_mode(chain.MODE_PLAIN)
-            vc.run_host(b)
-            vc.sync()
-            vc.capture_labels(ext=ext, max_event_clusters=weights.max_event_clusters if fallback else 0xFFFFFFFF)
-            vc.set_mode(chain.MODE_LABELS)
-            vc.run_host(b)
-            vc.sync()
-            add(name, b, vc.results(clusters=False))
+            res = vc.results(clusters=False)
+            add(name, b, res)
+            if mode == chain.MODE_PRUNED:
+                fallback += int(((res["status"] & chain.STATUS["mlp_fallback"]) != 0).sum())
+        if a < label_events:
+            for name, ext, fb in LABEL_FORMS:
+                vc.set_mode(chain.MODE_PLAIN)
+                vc.run_host(b)
+                vc.sync()
+                vc.capture_labels(ext=ext, max_event_clusters=weights.max_event_clusters if fb else 0xFFFFFFFF)
+                vc.set_mode(chain.MODE_LABELS)
+                vc.run_host(b)
+                vc.sync()
+                add(name, b, vc.results(clusters=False))
         vc.close()
     out = {}
     for name, r in rows.items():
         lr, lf, t, g, vr, vf = (sum(x[i] for x in r) for i in range(6))
         out[name] = {"long_efficiency": lf / max(1, lr), "ghost_rate": g / max(1, t), "velo_efficiency": vf / max(1, vr),
                      "tracks": t, "long_reconstructible": lr}
+        if name.startswith("labels"):
+            out[name]["events"] = min(n, label_events)
     out["events"] = n
+    out["fallback_events"] = fallback
     out["long_efficiency_loss"] = out["plain"]["long_efficiency"] - out["pruned"]["long_efficiency"]
     out["ghost_rate_change"] = out["pruned"]["ghost_rate"] - out["plain"]["ghost_rate"]
     return out
@@ -870,7 +881,7 @@ def main():
     ap.add_argument("--events", type=int, default=N_EVENTS, help="events per GPU (default: the 1,000,000 workload)")
     ap.add_argument("--cpu-sample", type=int, default=16384)
     ap.add_argument("--reference-sample", type=int, default=8192)
-    ap.add_argument("--quality-events", type=int, default=32768, help="MC-checked events of the workload head")
+    ap.add_argument("--quality-events", type=int, default=131072, help="MC-checked events of the workload head")
     ap.add_argument("--streams", type=int, default=2, help="contexts / streams that batches alternate between")
     ap.add_argument("--batch", type=int, default=BUCKET, help="events per batch (one CUDA graph per batch)")
     ap.add_argument("--weights", default=None, help="scorer weights (default: the committed file)")

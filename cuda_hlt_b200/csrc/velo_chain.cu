@@ -391,6 +391,13 @@ void size_decode_grid(VeloCtx* c)
   c->decode_blocks = static_cast<uint32_t>(std::max(1, occ) * c->sm_count);
 }
 
+void size_search_grid(VeloCtx* c)
+{
+  int occ = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, search_kernel<4>, 128, 0);
+  c->search_blocks = static_cast<uint32_t>(std::max(1, occ) * c->sm_count);
+}
+
 // A bounded wait that runs out: an mbarrier that nothing arrives on, waited for with
 // mbar_wait_parity (the wait of the scorer's copies and tensor-core steps) for `polls` polls;
 // the kernel then sets the error bit the scorer sets on a timeout and returns. Nothing is in
@@ -414,6 +421,29 @@ void drop_graphs(VeloCtx* c)
   }
   c->graphs.clear();
   c->lru.clear();
+}
+
+// The pruned mode's buffers (keep bits, candidate records, feature rows, hit slots: 45 bytes
+// per hit slot), allocated when the mode is first selected.
+int ensure_pruned_buffers(VeloCtx* c)
+{
+  if (c->d_keep) return 0;
+  bool ok = true;
+  ok &= dalloc(c->d_keep, c->hit_capacity) == cudaSuccess;
+  ok &= dalloc(c->d_cand_feat, (c->hit_capacity + kMlpTile) * kMlpK1 * 2) == cudaSuccess;
+  ok &= dalloc(c->d_cand_slot, c->hit_capacity) == cudaSuccess;
+  ok &= dalloc(c->d_cand_rec, c->hit_capacity) == cudaSuccess;
+  if (!ok) {
+    for (void* p : {static_cast<void*>(c->d_keep), static_cast<void*>(c->d_cand_feat),
+                    static_cast<void*>(c->d_cand_slot), static_cast<void*>(c->d_cand_rec)})
+      if (p) cudaFree(p);
+    c->d_keep = nullptr;
+    c->d_cand_feat = nullptr;
+    c->d_cand_slot = nullptr;
+    c->d_cand_rec = nullptr;
+    return VELO_ERR_CUDA;
+  }
+  return 0;
 }
 
 // Batch-size bucket of a graph: 1,024 events times a power of 4, at most the context's size.
@@ -470,10 +500,6 @@ int velo_create(const VeloConfig* cfg, const void* geometry, size_t geometry_byt
   ok &= dalloc(c->d_stage_id, 2 * c->hit_capacity) == cudaSuccess;
   ok &= dalloc(c->d_hit_size, c->hit_capacity) == cudaSuccess;
   ok &= dalloc(c->d_windows, c->hit_capacity) == cudaSuccess;
-  ok &= dalloc(c->d_keep, c->hit_capacity) == cudaSuccess;
-  ok &= dalloc(c->d_cand_feat, (c->hit_capacity + kMlpTile) * kMlpK1 * 2) == cudaSuccess;
-  ok &= dalloc(c->d_cand_slot, c->hit_capacity) == cudaSuccess;
-  ok &= dalloc(c->d_cand_rec, c->hit_capacity) == cudaSuccess;
   ok &= dalloc(c->d_module_start, static_cast<size_t>(N) * kModules) == cudaSuccess;
   ok &= dalloc(c->d_module_num, static_cast<size_t>(N) * kModules) == cudaSuccess;
   ok &= dalloc(c->d_event_hit_base, N) == cudaSuccess;
@@ -520,8 +546,7 @@ int velo_create(const VeloConfig* cfg, const void* geometry, size_t geometry_byt
     return fail(VELO_ERR_CUDA);
   int occ = 0;
   size_decode_grid(c);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, search_kernel<4>, 128, 0);
-  c->search_blocks = static_cast<uint32_t>(std::max(1, occ) * c->sm_count);
+  size_search_grid(c);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, gec_count_kernel, kGecThreads, 0);
   c->gec_blocks = static_cast<uint32_t>(std::max(1, occ) * c->sm_count);
   cudaFuncSetAttribute(search_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -541,6 +566,7 @@ int velo_create(const VeloConfig* cfg, const void* geometry, size_t geometry_byt
   const int score_per_sm = std::max(1, std::min(8, smem_sm / static_cast<int>(kScoreSmem + 1024)));
   c->score_blocks = static_cast<uint32_t>(score_per_sm * c->sm_count);
   c->mode = cfg->mode == VELO_MODE_PRUNED ? VELO_MODE_PRUNED : VELO_MODE_PLAIN;
+  if (c->mode == VELO_MODE_PRUNED && ensure_pruned_buffers(c) != 0) return fail(VELO_ERR_CUDA);
   // mapping: VELO_MAP_WARP keeps every event on warps, VELO_MAP_BLOCK on blocks; the
   // default splits at a cluster count (velo_set_block_threshold / the autotuner move it)
   c->block_threshold = cfg->mapping == VELO_MAP_WARP ? kEventHitCap : (cfg->mapping == VELO_MAP_BLOCK ? 0u : 1536u);
@@ -920,6 +946,11 @@ int velo_capture_labels(VeloCtx* c, int ext, uint32_t max_event_clusters)
 int velo_set_mode(VeloCtx* c, uint32_t mode)
 {
   if (!c || (mode != VELO_MODE_PLAIN && mode != VELO_MODE_PRUNED && mode != VELO_MODE_LABELS)) return VELO_ERR_INVALID;
+  if (mode == VELO_MODE_PRUNED) {
+    if (cudaSetDevice(c->device) != cudaSuccess) return VELO_ERR_CUDA;
+    const int rc = ensure_pruned_buffers(c);
+    if (rc) return rc;
+  }
   if (mode != c->mode) drop_graphs(c);
   c->mode = mode;
   return 0;
