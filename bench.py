@@ -543,7 +543,7 @@ def run_e2e(args, chunks, plan, local_rank, torch, world, dist, threshold, weigh
         o = chunks[ci].offsets[a:b + 1]
         offs.append(np.ascontiguousarray(o - o[0], dtype=np.uint64))
     max_batch_bytes = max(int(chunks[ci].offsets[b] - chunks[ci].offsets[a]) for ci, a, b in plan)
-    nctx = E2E_CONTEXTS
+    nctx = args.e2e_contexts
     ctxs = [chain.VeloChain(max_events=BUCKET, max_raw_bytes=max_batch_bytes + 4096, device=local_rank)
             for _ in range(nctx)]
     for vc in ctxs:
@@ -582,8 +582,10 @@ def run_e2e(args, chunks, plan, local_rank, torch, world, dist, threshold, weigh
                                                      C.c_void_p(s.cuda_stream)), "velo_download_async")
                 d2h[0] += nbytes
 
+    depth = max(1, min(args.e2e_depth, nctx - 1))  # batches in flight before the oldest is read back
+
     def step():
-        pending = None
+        pending = []
         for k, (ci, a, b) in enumerate(plan):
             vc, s = ctxs[k % nctx], streams[k % nctx]
             base = int(chunks[ci].offsets[a])
@@ -591,10 +593,11 @@ def run_e2e(args, chunks, plan, local_rank, torch, world, dist, threshold, weigh
             sub = events.EventBatch(chunks[ci].raw[base:base + nbytes], offs[k])
             vc.run_host(sub, s.cuda_stream)
             h2d[0] += nbytes + offs[k].nbytes
-            if pending is not None:
-                fetch(pending)
-            pending = k
-        fetch(pending)
+            pending.append(k)
+            if len(pending) > depth:
+                fetch(pending.pop(0))
+        for k in pending:
+            fetch(k)
         for s in streams:
             s.synchronize()
 
@@ -888,6 +891,10 @@ def main():
     ap.add_argument("--retrain", action="store_true", help="train the scorer here instead of loading it")
     ap.add_argument("--no-extras", action="store_true", help="skip the CPU baseline and reference-GPU legs")
     ap.add_argument("--no-ceiling", action="store_true", help="skip the per-stage / pruning-ceiling leg")
+    ap.add_argument("--e2e-contexts", type=int, default=E2E_CONTEXTS,
+                    help="contexts (and streams) in rotation in the end-to-end leg")
+    ap.add_argument("--e2e-depth", type=int, default=1,
+                    help="end-to-end leg: batches launched before the oldest is read back (< contexts)")
     ap.add_argument("--batched-events", type=int, default=500_000,
                     help="events of the nu ~ U(2,15) leg in 1k/4k/16k-event batches (0: skip)")
     ap.add_argument("--high-occ-events", type=int, default=200_000,

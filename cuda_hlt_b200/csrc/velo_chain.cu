@@ -157,7 +157,7 @@ cudaError_t dalloc(T*& p, size_t count)
 void free_all(VeloCtx* c)
 {
   void* ptrs[] = {c->d_labels, c->d_geometry, c->d_sp_patterns, c->d_sp_fx, c->d_sp_fy, c->d_sp_sizes, c->d_mlp_w, c->d_mlp_norm,
-                  c->d_hit_size, c->d_windows, c->d_keep, c->d_cand_feat, c->d_cand_slot, c->d_cand_rec, c->d_raw, c->d_raw_offsets, c->d_hxyzp,
+                  c->d_hit_size, c->d_windows, c->d_keep, c->d_cand_slot, c->d_cand_rec, c->d_raw, c->d_raw_offsets, c->d_hxyzp,
                   c->d_hid, c->d_stage_xyzp, c->d_stage_id, c->d_module_start, c->d_module_num, c->d_event_hit_base,
                   c->d_event_hits, c->d_status, c->d_track_n, c->d_track_hits, c->d_tracklets, c->d_weak, c->d_ttf,
                   c->d_event_tracks, c->d_event_track_hits, c->d_atomics, c->d_track_hit_number,
@@ -430,12 +430,14 @@ int ensure_pruned_buffers(VeloCtx* c)
   if (c->d_keep) return 0;
   bool ok = true;
   ok &= dalloc(c->d_keep, c->hit_capacity) == cudaSuccess;
-  ok &= dalloc(c->d_cand_feat, (c->hit_capacity + kMlpTile) * kMlpK1 * 2) == cudaSuccess;
+  // the feature rows share the decode kernel's staging area: decode has finished with it
+  // when candidate_features writes them, and the next run's decode starts after the scorer
+  c->d_cand_feat = reinterpret_cast<uint8_t*>(c->d_stage_xyzp);
   ok &= dalloc(c->d_cand_slot, c->hit_capacity) == cudaSuccess;
   ok &= dalloc(c->d_cand_rec, c->hit_capacity) == cudaSuccess;
   if (!ok) {
-    for (void* p : {static_cast<void*>(c->d_keep), static_cast<void*>(c->d_cand_feat),
-                    static_cast<void*>(c->d_cand_slot), static_cast<void*>(c->d_cand_rec)})
+    for (void* p : {static_cast<void*>(c->d_keep), static_cast<void*>(c->d_cand_slot),
+                    static_cast<void*>(c->d_cand_rec)})
       if (p) cudaFree(p);
     c->d_keep = nullptr;
     c->d_cand_feat = nullptr;
@@ -496,7 +498,9 @@ int velo_create(const VeloConfig* cfg, const void* geometry, size_t geometry_byt
   ok &= dalloc(c->d_run, 1) == cudaSuccess;
   ok &= dalloc(c->d_hxyzp, c->hit_capacity) == cudaSuccess;
   ok &= dalloc(c->d_hid, c->hit_capacity) == cudaSuccess;
-  ok &= dalloc(c->d_stage_xyzp, 2 * c->hit_capacity) == cudaSuccess;
+  // 2 records per hit slot; at least the pruned mode's feature rows, which share it
+  // ((hit slots + one tile) x 32 bytes)
+  ok &= dalloc(c->d_stage_xyzp, 2 * (c->hit_capacity + kMlpTile)) == cudaSuccess;
   ok &= dalloc(c->d_stage_id, 2 * c->hit_capacity) == cudaSuccess;
   ok &= dalloc(c->d_hit_size, c->hit_capacity) == cudaSuccess;
   ok &= dalloc(c->d_windows, c->hit_capacity) == cudaSuccess;

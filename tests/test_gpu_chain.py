@@ -434,3 +434,24 @@ def test_graph_per_bucket_serves_any_batch():
     vc.sync()
     _same_results(refs[0], vc.results(), batches[0].n_events, "after eviction")
     vc.close()
+
+
+def test_events_beyond_the_search_capacity():
+    """Events above the search's 16,384 clusters (pileup nu = 60: 17,300-18,300 clusters) are
+    flagged VELO_STATUS_HIT_OVERFLOW and keep no tracks; the events around them in the batch
+    are reconstructed as in a batch of their own."""
+    big = events.generate(seed=31, nu_min=60.0, nu_max=60.0, n_events=3, with_mc=False)
+    small = events.generate_config("batched_500k", n_events=4, first_event=600, with_mc=False)
+    parts = [small.event(0), big.event(0), small.event(1), big.event(1), small.event(2), big.event(2), small.event(3)]
+    raw = np.concatenate(parts)
+    offs = np.concatenate([[0], np.cumsum([p.size for p in parts])]).astype(np.uint64)
+    res = run_chain(events.EventBatch(raw, offs))
+    alone = run_chain(small)
+    n_hits = res["module_num"].reshape(-1, 52).sum(axis=1)
+    for pos in (1, 3, 5):
+        st = int(res["status"][pos])
+        assert n_hits[pos] > 16384, (pos, n_hits[pos])
+        assert st & chain.STATUS["hit_overflow"] and res["n_tracks"][pos] == 0, (pos, st)
+    for pos, e in ((0, 0), (2, 1), (4, 2), (6, 3)):
+        assert pu.canonical_tracks(chain.event_tracks(res, pos)) == pu.canonical_tracks(chain.event_tracks(alone, e))
+        assert res["status"][pos] == alone["status"][e]
