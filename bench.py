@@ -529,6 +529,47 @@ def run_ours(args, rank, world, local_rank):
     return result, chunks
 
 
+def host_link(torch, local_rank, nbytes=1 << 30, chunk=64 << 20, reps=3):
+    """Copy rates of this GPU's host link in GB/s: pinned host to device and device to host,
+    each alone and both at once (one stream per direction, 64 MB copies)."""
+    dev = torch.device("cuda", local_rank)
+    h_up = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    h_down = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    d_up = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    d_down = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    s_up, s_down = torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev)
+
+    def copies(dst, src, stream):
+        with torch.cuda.stream(stream):
+            for o in range(0, nbytes, chunk):
+                dst[o:o + chunk].copy_(src[o:o + chunk], non_blocking=True)
+
+    def rate(*jobs):
+        for job in jobs:
+            copies(*job)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            for job in jobs:
+                copies(*job)
+        torch.cuda.synchronize(dev)
+        return nbytes * reps / (time.perf_counter() - t0) / 1e9
+
+    up, down = (d_up, h_up, s_up), (h_down, d_down, s_down)
+    out = {"h2d_GBps": rate(up), "d2h_GBps": rate(down), "both_GBps_each_direction": rate(up, down)}
+    del h_up, h_down, d_up, d_down
+    return {k: round(v, 2) for k, v in out.items()}
+
+
+def link_bound(n_events, h2d_bytes, d2h_bytes, link):
+    """Events/s the host link allows for these bytes per step: both directions at the
+    concurrent rate while both have bytes to move, then the larger one alone."""
+    both = min(h2d_bytes, d2h_bytes) / (link["both_GBps_each_direction"] * 1e9)
+    rest_rate = link["h2d_GBps"] if h2d_bytes > d2h_bytes else link["d2h_GBps"]
+    rest = abs(h2d_bytes - d2h_bytes) / (rest_rate * 1e9)
+    return n_events / (both + rest)
+
+
 def run_e2e(args, chunks, plan, local_rank, torch, world, dist, threshold, weights, decode_warps=8):
     """velo_run_host from pinned memory, E2E_CONTEXTS contexts in rotation, each on its own
     stream, so that the upload of one batch, the kernels of the next and the read-back of a
@@ -565,9 +606,16 @@ def run_e2e(args, chunks, plan, local_rank, torch, world, dist, threshold, weigh
 
     d2h = [0]
     h2d = [0]
+    depth = max(1, min(args.e2e_depth, nctx - 1))  # batches in flight before the oldest is read back
+    # The batches of consecutive steps form one pipeline: a step's last read-backs overlap the
+    # next step's first uploads, and the pipeline drains once, at the end of the timed region
+    # (every step's uploads and read-backs still happen inside it).
+    pending = []  # (sequence number, batch) uploaded and launched, not yet read back
+    seq = [0]
 
-    def fetch(k):
-        vc, o, s = ctxs[k % nctx], outs[k % nctx], streams[k % nctx]
+    def fetch(item):
+        q, k = item
+        vc, o, s = ctxs[q % nctx], outs[q % nctx], streams[q % nctx]
         t, h, _ = vc.sync(clusters=False)
         n = plan[k][2] - plan[k][1]
         for buf, src, nbytes in ((o["atomics"], vc.out.atomics, 4 * (2 * n + 1)),
@@ -582,27 +630,29 @@ def run_e2e(args, chunks, plan, local_rank, torch, world, dist, threshold, weigh
                                                      C.c_void_p(s.cuda_stream)), "velo_download_async")
                 d2h[0] += nbytes
 
-    depth = max(1, min(args.e2e_depth, nctx - 1))  # batches in flight before the oldest is read back
-
     def step():
-        pending = []
         for k, (ci, a, b) in enumerate(plan):
-            vc, s = ctxs[k % nctx], streams[k % nctx]
+            q = seq[0]
+            seq[0] += 1
+            vc, s = ctxs[q % nctx], streams[q % nctx]
             base = int(chunks[ci].offsets[a])
             nbytes = int(chunks[ci].offsets[b]) - base
             sub = events.EventBatch(chunks[ci].raw[base:base + nbytes], offs[k])
             vc.run_host(sub, s.cuda_stream)
             h2d[0] += nbytes + offs[k].nbytes
-            pending.append(k)
+            pending.append((q, k))
             if len(pending) > depth:
                 fetch(pending.pop(0))
-        for k in pending:
-            fetch(k)
+
+    def drain():
+        while pending:
+            fetch(pending.pop(0))
         for s in streams:
             s.synchronize()
 
     for _ in range(max(1, args.warmup)):
         step()
+    drain()
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -610,6 +660,7 @@ def run_e2e(args, chunks, plan, local_rank, torch, world, dist, threshold, weigh
     t0 = time.perf_counter()
     for _ in range(args.steps):
         step()
+    drain()
     torch.cuda.synchronize()
     el = time.perf_counter() - t0
     if world > 1:
@@ -619,9 +670,16 @@ def run_e2e(args, chunks, plan, local_rank, torch, world, dist, threshold, weigh
     for c in chunks:
         cudart.cudaHostUnregister(c.raw.ctypes.data)
     n_events = sum(b - a for _, a, b in plan)
-    return {"value": n_events * world * args.steps / el, "unit": UNIT,
+    value = n_events * world * args.steps / el
+    link = host_link(torch, local_rank)
+    bound = world * link_bound(n_events, h2d[0] / args.steps, d2h[0] / args.steps, link)
+    return {"value": value, "unit": UNIT,
             "h2d_bytes_per_step": h2d[0] // args.steps, "d2h_bytes_per_step": d2h[0] // args.steps,
-            "timing": "host wall clock around K steps, synchronised", "contexts": nctx}
+            "timing": "host wall clock around K steps, synchronised; the batches of consecutive steps "
+                      "pipelined, drained at the end", "contexts": nctx, "depth": depth,
+            "host_link": {**link, "bound": bound, "frac": value / bound,
+                          "what": "events/s the measured host link allows for these bytes per step, "
+                                  "and the e2e value's fraction of it"}}
 
 
 # ---------------------------------------------------------------------------

@@ -93,7 +93,12 @@ struct VeloCtx {
   uint64_t *d_gec_ut_offsets = nullptr, *d_gec_scifi_offsets = nullptr;
   size_t gec_ut_cap = 0, gec_scifi_cap = 0;
   uint32_t gec_blocks = 0;
-  uint32_t* h_totals = nullptr;  // pinned [4]
+  uint32_t* h_totals = nullptr;  // pinned [4]: tracks, track hits, error bits of the last run
+  // pinned staging of host offsets (three slots of max_events + 1: raw, UT, SciFi) and the
+  // event that marks when the last copies out of it completed
+  uint64_t* h_offsets = nullptr;
+  cudaEvent_t ev_offsets = nullptr;
+  bool offsets_pending = false;
   cudaStream_t last_stream = nullptr;
   uint32_t last_n = 0;
   uint32_t launches = 0;
@@ -169,6 +174,8 @@ void free_all(VeloCtx* c)
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c->h_totals) cudaFreeHost(c->h_totals);
+  if (c->h_offsets) cudaFreeHost(c->h_offsets);
+  if (c->ev_offsets) cudaEventDestroy(c->ev_offsets);
   for (auto& kv : c->graphs) {
     cudaGraphExecDestroy(kv.second.exec);
     cudaGraphDestroy(kv.second.graph);
@@ -538,6 +545,10 @@ int velo_create(const VeloConfig* cfg, const void* geometry, size_t geometry_byt
   ok &= dalloc(c->d_block_events, N) == cudaSuccess;
   ok &= dalloc(c->d_event_order, N) == cudaSuccess;
   ok &= cudaMallocHost(reinterpret_cast<void**>(&c->h_totals), 4 * sizeof(uint32_t) + 8) == cudaSuccess;
+  ok &= cudaMallocHost(reinterpret_cast<void**>(&c->h_offsets), 3 * (static_cast<size_t>(N) + 1) * sizeof(uint64_t)) ==
+        cudaSuccess;
+  ok &= cudaEventCreateWithFlags(&c->ev_offsets, cudaEventDisableTiming) == cudaSuccess;
+  if (ok) std::memset(c->h_totals, 0, 4 * sizeof(uint32_t) + 8);
   if (!ok) return fail(VELO_ERR_CUDA);
   uint8_t pat[256], sizes[256];
   float fx[512], fy[512];
@@ -609,9 +620,9 @@ static int fill_outputs(VeloCtx* c, uint32_t n, VeloOutputs* out)
 
 // velo_run with or without the global event cut in front (gec: device inputs, or null), raw
 // offsets as u64 (raw_offsets) or u32 (raw_offsets32).
-static int run_chain(VeloCtx* c, const void* raw, const uint64_t* raw_offsets, const uint32_t* raw_offsets32,
-                     const VeloGecInput* gec, uint32_t n_events, void* stream, VeloOutputs* out,
-                     const uint32_t* event_list = nullptr, uint32_t n_raw = 0)
+static int launch_run(VeloCtx* c, const void* raw, const uint64_t* raw_offsets, const uint32_t* raw_offsets32,
+                      const VeloGecInput* gec, uint32_t n_events, void* stream, VeloOutputs* out,
+                      const uint32_t* event_list, uint32_t n_raw)
 {
   if (!c || (!raw && n_events) || (!raw_offsets && !raw_offsets32 && n_events)) return VELO_ERR_INVALID;
   if (gec && n_events && (!gec->ut_raw || !gec->ut_offsets || !gec->scifi_raw || !gec->scifi_offsets))
@@ -738,6 +749,26 @@ static int run_chain(VeloCtx* c, const void* raw, const uint64_t* raw_offsets, c
   return rc;
 }
 
+// Reads the run's totals (tracks, track hits, error bits) into the pinned h_totals on the
+// run's stream, queued right behind the run so that velo_sync only waits: a read queued at
+// sync time would wait behind whatever the caller queued on the stream's copy engine since.
+static int queue_totals(VeloCtx* c, cudaStream_t s, uint32_t n)
+{
+  VCK(cudaMemcpyAsync(c->h_totals, c->d_atomics + 2 * n, 4, cudaMemcpyDeviceToHost, s));
+  VCK(cudaMemcpyAsync(c->h_totals + 1, c->d_event_hit_offset + n, 4, cudaMemcpyDeviceToHost, s));
+  VCK(cudaMemcpyAsync(c->h_totals + 2, c->d_queue + 6, 4, cudaMemcpyDeviceToHost, s));
+  return 0;
+}
+
+static int run_chain(VeloCtx* c, const void* raw, const uint64_t* raw_offsets, const uint32_t* raw_offsets32,
+                     const VeloGecInput* gec, uint32_t n_events, void* stream, VeloOutputs* out,
+                     const uint32_t* event_list = nullptr, uint32_t n_raw = 0)
+{
+  const int rc = launch_run(c, raw, raw_offsets, raw_offsets32, gec, n_events, stream, out, event_list, n_raw);
+  if (rc) return rc;
+  return queue_totals(c, static_cast<cudaStream_t>(stream), n_events);
+}
+
 int velo_run(VeloCtx* c, const void* raw, const uint64_t* raw_offsets, uint32_t n_events, void* stream,
              VeloOutputs* out)
 {
@@ -766,22 +797,35 @@ int velo_run_gec(VeloCtx* c, const void* raw, const uint64_t* raw_offsets, const
   return run_chain(c, raw, raw_offsets, nullptr, gec, n_events, stream, out);
 }
 
+// Host offsets go through the context's pinned staging (rebased on the way), so that their
+// copy is asynchronous whatever memory the caller's offsets live in: a copy from pageable
+// memory may wait for the stream's earlier work. begin_upload waits until the previous run's
+// copies out of the staging have completed (long before, in a pipeline); end_upload marks them.
+static int begin_upload(VeloCtx* c)
+{
+  if (c->offsets_pending) VCK(cudaEventSynchronize(c->ev_offsets));
+  c->offsets_pending = false;
+  return 0;
+}
+
+static int end_upload(VeloCtx* c, cudaStream_t s)
+{
+  VCK(cudaEventRecord(c->ev_offsets, s));
+  c->offsets_pending = true;
+  return 0;
+}
+
 // Copies a host batch (bytes from offsets[0] to offsets[n], offsets[n + 1]) to device buffers,
-// rebasing the offsets when the batch does not start at byte 0.
-static int upload_batch(const void* raw_host, const uint64_t* offsets_host, uint32_t n, uint8_t* d_raw,
-                        uint64_t* d_offsets, cudaStream_t s)
+// with the offsets rebased to the batch's first byte through staging slot `slot`.
+static int upload_batch(VeloCtx* c, const void* raw_host, const uint64_t* offsets_host, uint32_t n, uint8_t* d_raw,
+                        uint64_t* d_offsets, cudaStream_t s, int slot)
 {
   const uint64_t first = offsets_host[0];
   const uint64_t bytes = offsets_host[n] - first;
   VCK(cudaMemcpyAsync(d_raw, static_cast<const uint8_t*>(raw_host) + first, bytes, cudaMemcpyHostToDevice, s));
-  if (first == 0) {
-    VCK(cudaMemcpyAsync(d_offsets, offsets_host, 8ull * (n + 1), cudaMemcpyHostToDevice, s));
-  } else {
-    std::vector<uint64_t> rebased(offsets_host, offsets_host + n + 1);
-    for (auto& v : rebased) v -= first;
-    VCK(cudaMemcpyAsync(d_offsets, rebased.data(), 8ull * (n + 1), cudaMemcpyHostToDevice, s));
-    VCK(cudaStreamSynchronize(s));
-  }
+  uint64_t* staged = c->h_offsets + static_cast<size_t>(slot) * (c->cfg.max_events + 1);
+  for (uint32_t i = 0; i <= n; ++i) staged[i] = offsets_host[i] - first;
+  VCK(cudaMemcpyAsync(d_offsets, staged, 8ull * (n + 1), cudaMemcpyHostToDevice, s));
   return 0;
 }
 
@@ -813,11 +857,14 @@ int velo_run_gec_host(VeloCtx* c, const void* raw_host, const uint64_t* raw_offs
   const uint64_t scifi_bytes = gec_host->scifi_offsets[n_events] - gec_host->scifi_offsets[0];
   int rc = ensure_staging(c, c->d_gec_ut, c->gec_ut_cap, ut_bytes);
   if (rc == 0) rc = ensure_staging(c, c->d_gec_scifi, c->gec_scifi_cap, scifi_bytes);
-  if (rc == 0) rc = upload_batch(raw_host, raw_offsets_host, n_events, c->d_raw, c->d_raw_offsets, s);
-  if (rc == 0) rc = upload_batch(gec_host->ut_raw, gec_host->ut_offsets, n_events, c->d_gec_ut, c->d_gec_ut_offsets, s);
+  if (rc == 0) rc = begin_upload(c);
+  if (rc == 0) rc = upload_batch(c, raw_host, raw_offsets_host, n_events, c->d_raw, c->d_raw_offsets, s, 0);
   if (rc == 0)
-    rc = upload_batch(gec_host->scifi_raw, gec_host->scifi_offsets, n_events, c->d_gec_scifi,
-                      c->d_gec_scifi_offsets, s);
+    rc = upload_batch(c, gec_host->ut_raw, gec_host->ut_offsets, n_events, c->d_gec_ut, c->d_gec_ut_offsets, s, 1);
+  if (rc == 0)
+    rc = upload_batch(c, gec_host->scifi_raw, gec_host->scifi_offsets, n_events, c->d_gec_scifi,
+                      c->d_gec_scifi_offsets, s, 2);
+  if (rc == 0) rc = end_upload(c, s);
   if (rc) return rc;
   const VeloGecInput dev{c->d_gec_ut, c->d_gec_ut_offsets, c->d_gec_scifi, c->d_gec_scifi_offsets,
                          gec_host->max_clusters};
@@ -825,21 +872,18 @@ int velo_run_gec_host(VeloCtx* c, const void* raw_host, const uint64_t* raw_offs
 }
 
 // Copies a host batch with u32 offsets (bytes from offsets[0] to offsets[n]) to the
-// context's device buffers, rebasing the offsets when the batch does not start at byte 0.
+// context's device buffers, the offsets rebased through the pinned staging.
 static int upload_batch_u32(VeloCtx* c, const void* raw_host, const uint32_t* offsets_host, uint32_t n, cudaStream_t s)
 {
   const uint32_t first = offsets_host[0];
   const uint64_t bytes = static_cast<uint64_t>(offsets_host[n]) - first;
+  int rc = begin_upload(c);
+  if (rc) return rc;
   VCK(cudaMemcpyAsync(c->d_raw, static_cast<const uint8_t*>(raw_host) + first, bytes, cudaMemcpyHostToDevice, s));
-  if (first == 0) {
-    VCK(cudaMemcpyAsync(c->d_raw_offsets32, offsets_host, 4ull * (n + 1), cudaMemcpyHostToDevice, s));
-  } else {
-    std::vector<uint32_t> rebased(offsets_host, offsets_host + n + 1);
-    for (auto& v : rebased) v -= first;
-    VCK(cudaMemcpyAsync(c->d_raw_offsets32, rebased.data(), 4ull * (n + 1), cudaMemcpyHostToDevice, s));
-    VCK(cudaStreamSynchronize(s));
-  }
-  return 0;
+  uint32_t* staged = reinterpret_cast<uint32_t*>(c->h_offsets);
+  for (uint32_t i = 0; i <= n; ++i) staged[i] = offsets_host[i] - first;
+  VCK(cudaMemcpyAsync(c->d_raw_offsets32, staged, 4ull * (n + 1), cudaMemcpyHostToDevice, s));
+  return end_upload(c, s);
 }
 
 int velo_run_host_u32(VeloCtx* c, const void* raw_host, const uint32_t* raw_offsets_host, uint32_t n_events,
@@ -864,7 +908,9 @@ int velo_run_host(VeloCtx* c, const void* raw_host, const uint64_t* raw_offsets_
   if (raw_offsets_host[n_events] - raw_offsets_host[0] > c->cfg.max_raw_bytes) return VELO_ERR_CAPACITY;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (cudaSetDevice(c->device) != cudaSuccess) return VELO_ERR_CUDA;
-  const int rc = upload_batch(raw_host, raw_offsets_host, n_events, c->d_raw, c->d_raw_offsets, s);
+  int rc = begin_upload(c);
+  if (rc == 0) rc = upload_batch(c, raw_host, raw_offsets_host, n_events, c->d_raw, c->d_raw_offsets, s, 0);
+  if (rc == 0) rc = end_upload(c, s);
   if (rc) return rc;
   return velo_run(c, c->d_raw, c->d_raw_offsets, n_events, stream, out);
 }
@@ -875,12 +921,7 @@ int velo_sync(VeloCtx* c, uint32_t* total_tracks, uint32_t* total_track_hits, ui
   if (cudaSetDevice(c->device) != cudaSuccess) return VELO_ERR_CUDA;
   cudaStream_t s = c->last_stream;
   const uint32_t N = c->last_n;
-  if (total_tracks || total_track_hits) {
-    VCK(cudaMemcpyAsync(c->h_totals, c->d_atomics + 2 * N, 4, cudaMemcpyDeviceToHost, s));
-    VCK(cudaMemcpyAsync(c->h_totals + 1, c->d_event_hit_offset + N, 4, cudaMemcpyDeviceToHost, s));
-  }
-  VCK(cudaMemcpyAsync(c->h_totals + 2, c->d_queue + 6, 4, cudaMemcpyDeviceToHost, s));
-  VCK(cudaStreamSynchronize(s));
+  VCK(cudaStreamSynchronize(s));  // the totals were queued behind the run
   if (c->h_totals[2]) return VELO_ERR_DEVICE_TIMEOUT;
   if (total_tracks) *total_tracks = c->h_totals[0];
   if (total_track_hits) *total_track_hits = c->h_totals[1];
@@ -1057,6 +1098,7 @@ int velo_check_wait_timeout(VeloCtx* c, uint32_t polls, void* stream)
   VCK(cudaMemsetAsync(c->d_queue + 6, 0, sizeof(uint32_t), s));
   wait_timeout_kernel<<<1, 32, 0, s>>>(c->d_queue + 6, polls);
   VCK(cudaGetLastError());
+  VCK(cudaMemcpyAsync(c->h_totals + 2, c->d_queue + 6, 4, cudaMemcpyDeviceToHost, s));  // read by velo_sync
   return 0;
 }
 

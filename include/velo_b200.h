@@ -24,7 +24,8 @@
  *
  * Conventions: every entry point returns 0 or a negative VELO_ERR_* code and never throws.
  * Device pointers are plain addresses; streams are cudaStream_t passed as void*. Nothing
- * blocks except velo_sync. A context is used by one host thread at a time; separate
+ * blocks except velo_sync (and the host-buffer runs, until the previous run's offsets have
+ * left the staging buffer). A context is used by one host thread at a time; separate
  * contexts may run concurrently on separate streams.
  */
 #ifndef VELO_B200_H
@@ -245,8 +246,12 @@ int velo_create(const VeloConfig* cfg, const void* geometry, size_t geometry_byt
 int velo_run(VeloCtx* ctx, const void* raw, const uint64_t* raw_offsets, uint32_t n_events, void* stream,
              VeloOutputs* out);
 
-/* Same, from host buffers (pinned for overlap): copies the input to the context's device
- * buffers on the stream, then runs. */
+/* Same, from host buffers: copies the input to the context's device buffers on the stream,
+ * then runs. The raw bytes are copied straight from raw_host (pin or register it for the copy
+ * to overlap other work); the offsets go through a pinned staging buffer of the context,
+ * rebased to the batch's first byte on the way, so their copy is asynchronous whatever memory
+ * they are in. The call waits only if the previous host run's offsets have not yet left that
+ * buffer. */
 int velo_run_host(VeloCtx* ctx, const void* raw_host, const uint64_t* raw_offsets_host, uint32_t n_events,
                   void* stream, VeloOutputs* out);
 
@@ -292,7 +297,9 @@ int velo_run_gec(VeloCtx* ctx, const void* raw, const uint64_t* raw_offsets, con
 int velo_run_gec_host(VeloCtx* ctx, const void* raw_host, const uint64_t* raw_offsets_host,
                       const VeloGecInput* gec_host, uint32_t n_events, void* stream, VeloOutputs* out);
 
-/* Waits for the context's last run; fills totals (tracks, track hits, clusters). */
+/* Waits for the context's last run (its stream); fills totals (tracks, track hits, clusters).
+ * The track and track-hit totals are read into pinned memory at the end of every run, so the
+ * wait does not queue behind copies issued on the stream's copy engine since. */
 int velo_sync(VeloCtx* ctx, uint32_t* total_tracks, uint32_t* total_track_hits, uint64_t* total_clusters);
 
 /* ---- learned seed/extension scorer (no counterpart in the reference) ----
