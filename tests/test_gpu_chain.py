@@ -364,6 +364,30 @@ def test_u32_offsets_equal_u64():
     vc.close()
 
 
+def test_host_offsets_staging():
+    """velo_run_host stages the caller's offsets through pinned memory of the context,
+    rebased to the batch's first byte: a batch that starts inside the caller's buffer equals
+    the same events run alone, also when it follows another host run on the same stream
+    without a wait in between (the staging is reused only once the previous copy is done),
+    and the totals velo_sync reports are the last run's."""
+    b = events.generate_config("batched_500k", n_events=120, first_event=700)
+    sub = b.subset(20, 120)
+    ref_sub = run_chain(sub)
+    vc = chain.VeloChain(max_events=b.n_events, max_raw_bytes=int(b.raw.size) + 4096)
+    rebased = events.EventBatch(b.raw, np.ascontiguousarray(b.offsets[20:]))
+    vc.run_host(rebased)
+    t, h, _ = vc.sync(clusters=False)
+    _same_results(ref_sub, vc.results(), sub.n_events, "host u64, rebased")
+    assert t == int(ref_sub["atomics"][2 * sub.n_events]) and h == len(ref_sub["hit_id"])
+    for _ in range(2):
+        vc.run_host(b)
+        vc.run_host(rebased)
+    t, h, _ = vc.sync(clusters=False)
+    _same_results(ref_sub, vc.results(), sub.n_events, "host u64, rebased, after another run")
+    assert t == int(ref_sub["atomics"][2 * sub.n_events]) and h == len(ref_sub["hit_id"])
+    vc.close()
+
+
 def test_selected_events_u32():
     """velo_run_selected_u32 decodes the caller's selection (Allen's dev_event_list after
     global_event_cut_t): position i holds raw event list[i], equal to a run over those events
