@@ -209,10 +209,11 @@ struct EventScratch {
 };
 
 // Seeding windows read from the fill_candidates output: {h0 first | last << 16, h2 first |
-// last << 16} per hit, event-relative (0xFFFF: no window).
+// last << 16} per hit, event-relative (0xFFFF: no window). Each is read once per event, so
+// it is loaded evict-first: the cache keeps the cluster records, which the search rereads.
 struct StoredWindows {
   const uint2* w;
-  __device__ __forceinline__ uint2 operator()(uint32_t h1, uint32_t) const { return w[h1]; }
+  __device__ __forceinline__ uint2 operator()(uint32_t h1, uint32_t) const { return __ldcs(w + h1); }
 };
 
 // Seeding windows computed where they are needed, with the searches of fill_candidates
