@@ -346,7 +346,7 @@ int launch_chain(VeloCtx* c, const ChainPointers& P, const GecPointers* G, cudaS
   } else if (pruned) {
     candidate_features_kernel<<<c->feature_blocks, kFillThreads, 0, s>>>(P);
     VCK(cudaGetLastError());
-    score_candidates_kernel<<<c->score_blocks, kMlpTile, kScoreSmem, s>>>(P);
+    score_candidates_kernel<<<c->score_blocks, kScoreThreads, kScoreSmem, s>>>(P);
     c->launches += 2;
   }
   VCK(cudaGetLastError());
@@ -573,12 +573,13 @@ int velo_create(const VeloConfig* cfg, const void* geometry, size_t geometry_byt
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, candidate_features_kernel, kFillThreads, 0);
   c->feature_blocks = static_cast<uint32_t>(std::max(1, occ) * c->sm_count);
   // the scorer: as many CTAs per SM as shared memory holds (1 KB of it is reserved per
-  // block), at most 8 (each holds 64 of the SM's 512 tensor-memory columns)
+  // block), at most 4 (each holds 128 of the SM's 512 tensor-memory columns)
   cudaFuncSetAttribute(score_candidates_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        static_cast<int>(kScoreSmem));
   int smem_sm = 0;
   cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c->device);
-  const int score_per_sm = std::max(1, std::min(8, smem_sm / static_cast<int>(kScoreSmem + 1024)));
+  const int score_per_sm =
+    std::max(1, std::min(static_cast<int>(512 / kScoreTmemCols), smem_sm / static_cast<int>(kScoreSmem + 1024)));
   c->score_blocks = static_cast<uint32_t>(score_per_sm * c->sm_count);
   c->mode = cfg->mode == VELO_MODE_PRUNED ? VELO_MODE_PRUNED : VELO_MODE_PLAIN;
   if (c->mode == VELO_MODE_PRUNED && ensure_pruned_buffers(c) != 0) return fail(VELO_ERR_CUDA);

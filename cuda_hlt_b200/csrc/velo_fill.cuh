@@ -7,9 +7,10 @@
 //                          computes its twelve proxy-triplet features and writes them,
 //                          normalised and in bf16, as a row of 128-row tiles laid out for
 //                          the tensor core, with the candidate's hit slot alongside;
-//   score_candidates       a persistent tcgen05 kernel: each CTA bulk-copies 4 KB tiles of
-//                          those rows into a four-slot shared-memory ring, runs the MLP and
-//                          writes the verdict per candidate: a pruned seed gets its h0 window
+//   score_candidates       a persistent tcgen05 kernel: each CTA bulk-copies pairs of 4 KB
+//                          tiles of those rows into a shared-memory ring, runs the MLP's
+//                          three layers on the tensor core for both tiles at once and writes
+//                          the verdict per candidate: a pruned seed gets its h0 window
 //                          cleared, so the search never sees it; keep bits per hit (bit 0
 //                          seed keep, bit 1 extension keep) are kept for the outputs.
 // Events above the scorer's occupancy range append no candidates (the plain search) and get
@@ -44,51 +45,120 @@ __global__ void __launch_bounds__(kFillThreads) candidate_features_kernel(ChainP
   }
 }
 
-// Shared memory of score_candidates: the inference tile buffers (whose X tile is slot 0 of
-// the copy ring) plus kScoreRing - 1 more X tiles, each slot with its barrier. Tiles are
-// prefetched kScoreRing - 1 ahead, so every CTA keeps several 4 KB copies in flight.
-constexpr uint32_t kScoreRing = 4;
+// score_candidates: 256 threads, two 128-row tiles per iteration. Warps 0-3 hold the rows of
+// the first tile, warps 4-7 those of the second (a warp reads the TMEM lanes 32 * (warp % 4)
+// onwards, so both halves read their own tile's accumulators, 64 columns apart): one barrier
+// round and one tensor-core round trip per layer serve two tiles. All three layers run on
+// the tensor core, in the training kernel's layouts: hidden tiles 80 wide with a ones column,
+// so the layer-2 and head biases come out of the MMAs, and each epilogue is ReLU, round to
+// bf16 and store; the logits are the first two columns of the head's accumulators. Tile
+// pairs are bulk-copied (8 KB, contiguous in the candidate list) into a two-deep ring, one
+// pair ahead; the epilogues take their accumulators 16 columns at a time, so three CTAs fit
+// on an SM without spilling.
+constexpr uint32_t kScorePair = 2;                                  // tiles per iteration
+constexpr uint32_t kScoreThreads = kMlpTile * kScorePair;           // 256
+constexpr uint32_t kScoreRing = 2;                                  // tile pairs in the ring
+constexpr uint32_t kScoreTmemCols = kMlpHidden * kScorePair;        // 128
 struct __align__(128) ScoreSmem {
-  MlpInferSmem mlp;
-  uint8_t x[kScoreRing - 1][kCandTileBytes];
+  uint8_t w1[kMlpW1 * 2];                          // W1 [64][16]
+  uint8_t w2[kMlpW2 * 2];                          // W2 [64][80], bias in column 64
+  uint8_t w3[kMlpW3 * 2];                          // W3 [16][80], rows 2..15 zero
+  uint8_t x[kScoreRing][kScorePair * kCandTileBytes];
+  uint8_t h[kScorePair][kMlpTile * kMlpK2 * 2];    // H1, then H2: [128][80], 1.0 in column 64
   uint64_t load_bar[kScoreRing];
+  uint64_t mbar;
+  uint32_t tmem;
 };
 constexpr uint32_t kScoreSmem = sizeof(ScoreSmem) + 128;
 
-__global__ void __launch_bounds__(kMlpTile) score_candidates_kernel(ChainPointers P)
+// This thread's row of a tile pair: half (0/1) picks the tile, row its row in it.
+__device__ __forceinline__ uint32_t score_half() { return threadIdx.x >> 7; }
+__device__ __forceinline__ uint32_t score_row() { return threadIdx.x & (kMlpTile - 1); }
+
+// Epilogue of a hidden layer for this thread's row: ReLU of the 64 accumulators, rounded to
+// bf16 into columns 0..63 of the row of H (the ones column stays).
+__device__ __forceinline__ void score_hidden_epilogue(uint8_t* h, uint32_t taddr_row, uint32_t row)
+{
+#pragma unroll
+  for (uint32_t c = 0; c < 4; ++c) {
+    float v[16];
+    tmem_ld16(taddr_row + 16 * c, v);
+    tmem_ld_wait();
+#pragma unroll
+    for (uint32_t u = 0; u < 2; ++u) {
+      uint4 q;
+      q.x = pack_bf16x2(fmaxf(v[8 * u + 0], 0.f), fmaxf(v[8 * u + 1], 0.f));
+      q.y = pack_bf16x2(fmaxf(v[8 * u + 2], 0.f), fmaxf(v[8 * u + 3], 0.f));
+      q.z = pack_bf16x2(fmaxf(v[8 * u + 4], 0.f), fmaxf(v[8 * u + 5], 0.f));
+      q.w = pack_bf16x2(fmaxf(v[8 * u + 6], 0.f), fmaxf(v[8 * u + 7], 0.f));
+      *reinterpret_cast<uint4*>(h + canon_off(row, 2 * c + u, kSbo2)) = q;
+    }
+  }
+}
+
+// One layer on both tiles of the pair: D(half j) = A_j * B^T into TMEM columns 64 j.., then
+// wait. False (uniformly) on timeout.
+__device__ __forceinline__ bool score_layer(ScoreSmem& s, uint32_t& phase, const uint8_t* a0, const uint8_t* a1,
+                                            uint32_t a_sbo, const uint8_t* b, uint32_t b_sbo, uint32_t k, uint32_t n)
+{
+  umma_stage_barrier();
+  if (threadIdx.x == 0) {
+    umma_issue(s.tmem, a0, a_sbo, b, b_sbo, k, n, false);
+    umma_issue(s.tmem + kMlpHidden, a1, a_sbo, b, b_sbo, k, n, false);
+    umma_commit(&s.mbar);
+  }
+  return umma_wait(&s.mbar, phase);
+}
+
+__global__ void __launch_bounds__(kScoreThreads, 3) score_candidates_kernel(ChainPointers P)
 {
   extern __shared__ uint8_t s_dyn[];
   ScoreSmem& s = *reinterpret_cast<ScoreSmem*>((reinterpret_cast<uintptr_t>(s_dyn) + 127) & ~uintptr_t(127));
   const uint32_t rows = P.queue[7];
   const uint32_t tiles = (rows + kMlpTile - 1) / kMlpTile;
-  if (blockIdx.x >= tiles) return;  // uniform: this CTA has no tile
-  if (threadIdx.x == 0)
+  const uint32_t pairs = (tiles + kScorePair - 1) / kScorePair;
+  if (blockIdx.x >= pairs) return;  // uniform: this CTA has no tile
+  // set-up: tensor memory, barriers, weights (as mlp_infer_setup, for the pair layout)
+  if (threadIdx.x < 32) tmem_alloc(&s.tmem, kScoreTmemCols);
+  if (threadIdx.x == 0) {
+    mbar_init1(&s.mbar);
     for (uint32_t i = 0; i < kScoreRing; ++i) mbar_init1(&s.load_bar[i]);
-  mlp_infer_setup(s.mlp, P.mlp);  // includes the barrier that publishes the inits
-  uint8_t* xbuf[kScoreRing];
-  xbuf[0] = s.mlp.x;
-  for (uint32_t i = 1; i < kScoreRing; ++i) xbuf[i] = s.x[i - 1];
+  }
+  load_canon(s.w1, P.mlp.w, kMlpHidden, kMlpK1);
+  load_canon(s.w2, P.mlp.w + kMlpW1, kMlpHidden, kMlpK2);
+  load_canon(s.w3, P.mlp.w + kMlpW1 + kMlpW2, kMlpOutPad, kMlpK2);
+  // columns 64..79 of both H tiles: 1.0 (the bias column), then zeros; never overwritten
+  for (uint32_t c = threadIdx.x; c < kScorePair * kMlpTile * 2; c += blockDim.x) {
+    const uint32_t t = c / (2 * kMlpTile), row = (c / 2) % kMlpTile, kb = 8 + c % 2;
+    const uint4 v = kb == 8 ? make_uint4(pack_bf16x2(1.f, 0.f), 0u, 0u, 0u) : make_uint4(0u, 0u, 0u, 0u);
+    *reinterpret_cast<uint4*>(s.h[t] + canon_off(row, kb, kSbo2)) = v;
+  }
+  umma_stage_barrier();  // publishes the barrier inits, the weights and the TMEM address
+
+  // pair p (tiles 2p, 2p + 1) is 8 KB at tile 2p; the last pair may hold one tile
+  auto issue_load = [&](uint32_t pair, uint32_t slot) {
+    const uint32_t t0 = pair * kScorePair;
+    const uint32_t n = min(kScorePair, tiles - t0);
+    bulk_load_smem(s.x[slot], P.cand_feat + static_cast<size_t>(t0) * kCandTileBytes, n * kCandTileBytes,
+                   &s.load_bar[slot]);
+  };
   uint32_t mma_phase = 0, load_phase = 0;  // load_phase: bit i = parity of slot i
   bool ok = true;
-  // this CTA's tiles are blockIdx.x + k * gridDim.x, k = 0, 1, ...; tile k goes to slot k % ring
+  // this CTA's pairs are blockIdx.x + k * gridDim.x; pair k goes to slot k % ring
   if (threadIdx.x == 0)
     for (uint32_t k = 0; k + 1 < kScoreRing; ++k) {
-      const uint32_t t = blockIdx.x + k * gridDim.x;
-      if (t < tiles)
-        bulk_load_smem(xbuf[k], P.cand_feat + static_cast<size_t>(t) * kCandTileBytes, kCandTileBytes,
-                       &s.load_bar[k]);
+      const uint32_t p = blockIdx.x + k * gridDim.x;
+      if (p < pairs) issue_load(p, k);
     }
+  const uint32_t half = score_half(), row = score_row();
+  const uint32_t taddr_row = s.tmem + (((threadIdx.x >> 5) & 3u) * 32u << 16) + half * kMlpHidden;
   uint32_t k = 0;
-  for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++k) {
+  for (uint32_t pair = blockIdx.x; pair < pairs; pair += gridDim.x, ++k) {
     const uint32_t slot = k % kScoreRing;
-    // refill the slot used by tile k - 1 (its MMAs are complete) with tile k + ring - 1
-    const uint32_t ahead = tile + (kScoreRing - 1) * gridDim.x;
-    if (threadIdx.x == 0 && ahead < tiles) {
-      const uint32_t as = (k + kScoreRing - 1) % kScoreRing;
-      bulk_load_smem(xbuf[as], P.cand_feat + static_cast<size_t>(ahead) * kCandTileBytes, kCandTileBytes,
-                     &s.load_bar[as]);
-    }
-    const uint32_t r = tile * kMlpTile + threadIdx.x;
+    // refill the slot that pair k - 1 used (its MMAs are complete) with pair k + ring - 1
+    const uint32_t ahead = pair + (kScoreRing - 1) * gridDim.x;
+    if (threadIdx.x == 0 && ahead < pairs) issue_load(ahead, (k + kScoreRing - 1) % kScoreRing);
+    const uint32_t r = (pair * kScorePair + half) * kMlpTile + row;
     const uint32_t hit = r < rows ? P.cand_slot[r] : 0u;  // issued early: used after the MMAs
     const bool loaded = mbar_wait_parity(&s.load_bar[slot], (load_phase >> slot) & 1u);
     load_phase ^= 1u << slot;
@@ -96,11 +166,24 @@ __global__ void __launch_bounds__(kMlpTile) score_candidates_kernel(ChainPointer
       ok = false;
       break;
     }
-    float z0 = 0.f, z1 = 0.f;
-    if (!mlp_tile_forward(s.mlp, mma_phase, z0, z1, xbuf[slot])) {
+    if (!score_layer(s, mma_phase, s.x[slot], s.x[slot] + kCandTileBytes, kSbo1, s.w1, kSbo1, kMlpK1, kMlpHidden)) {
       ok = false;
       break;
     }
+    score_hidden_epilogue(s.h[half], taddr_row, row);  // H1
+    if (!score_layer(s, mma_phase, s.h[0], s.h[1], kSbo2, s.w2, kSbo2, kMlpK2, kMlpHidden)) {
+      ok = false;
+      break;
+    }
+    score_hidden_epilogue(s.h[half], taddr_row, row);  // H2, over H1 (layer 2 has read it)
+    if (!score_layer(s, mma_phase, s.h[0], s.h[1], kSbo2, s.w3, kSbo2, kMlpK2, kMlpOutPad)) {
+      ok = false;
+      break;
+    }
+    float z[16];
+    tmem_ld16(taddr_row, z);
+    tmem_ld_wait();
+    const float z0 = z[0], z1 = z[1];
     if (r < rows) {
       const bool seed = z0 >= P.mlp.seed_logit;
       const bool ext = !P.mlp.use_ext || z1 >= P.mlp.ext_logit;
@@ -114,7 +197,10 @@ __global__ void __launch_bounds__(kMlpTile) score_candidates_kernel(ChainPointer
     // whose issued copy has not been consumed
     for (uint32_t j = 0; j < kScoreRing; ++j) mbar_wait_parity(&s.load_bar[j], (load_phase >> j) & 1u);
   }
-  mlp_infer_teardown(s.mlp);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (threadIdx.x < 32) tmem_dealloc(s.tmem, kScoreTmemCols);
 }
 
 }  // namespace velo

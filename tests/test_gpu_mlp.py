@@ -185,6 +185,47 @@ def test_pruned_without_pruning_is_plain():
         assert np.array_equal(fb["states"][k], plain["states"][k])
 
 
+def test_score_kernel_verdicts_match_oracle():
+    """The verdicts of score_candidates (bit 0 of the keep bits of every scored seed: kept or
+    pruned) equal the oracle's forward pass on the oracle's features of the same clusters,
+    wherever the logit clears the threshold by more than fp32 summation-order noise. Every
+    event and every candidate is scored (no gates), over many 256-row tile pairs, the last
+    of them partial; the threshold sits at the median logit, so half the seeds go."""
+    b = events.generate(seed=14, nu_min=2.0, nu_max=15.0, n_events=48, with_mc=False)
+    d = random_weights(15)
+    d["min_pairs"] = 0
+    d["min_event_clusters"] = 0
+    plain = run_mode(b, chain.MODE_PLAIN)  # the clusters are the same in both modes
+    per_event = []
+    for e in range(b.n_events):
+        mods = chain.event_clusters(plain, e)
+        cat = {k: np.concatenate([m[k] for m in mods]) for k in ("x", "y", "z", "phi", "size")}
+        idx, _, fo = mlp_oracle.event_features(cat["x"], cat["y"], cat["z"], cat["phi"], cat["size"],
+                                               [len(m["x"]) for m in mods])
+        per_event.append((idx, mlp_oracle.forward_bf16(fo, d)[0][:, 0] if len(idx) else np.zeros(0, np.float32)))
+    z_all = np.concatenate([z for _, z in per_event])
+    cut = float(np.median(z_all))
+    d["seed_threshold"] = float(np.float32(1.0 / (1.0 + np.exp(-cut))))
+    res = run_mode(b, chain.MODE_PRUNED, mlp.dict_to_weights(d))
+    ms = res["module_start"].reshape(-1, 52)
+    scale = 1.0 + np.abs(z_all).max()
+    total = clear = mismatched = kept = 0
+    for e, (idx, z) in enumerate(per_event):
+        if len(idx) == 0:
+            continue
+        verdict = (res["cluster_keep"][int(ms[e, 0]) + idx] & 1).astype(bool)
+        far = np.abs(z - cut) > 1e-2 * scale
+        total += len(idx)
+        clear += int(far.sum())
+        mismatched += int((verdict[far] != (z[far] >= cut)).sum())
+        kept += int(verdict.sum())
+    assert total > 20_000 and clear > 0.8 * total, (total, clear)
+    assert 0.3 * total < kept < 0.7 * total, (kept, total)
+    # they agree except where the device picked the other proxy pair of a near-tie
+    # (fast-math division: a few rows in a thousand)
+    assert mismatched <= 0.005 * clear, (mismatched, clear)
+
+
 def test_scoring_gate():
     b = events.generate(seed=12, nu_min=2.0, nu_max=15.0, n_events=64, with_mc=False)
     ref = canonical(run_mode(b, chain.MODE_PLAIN), b.n_events)
