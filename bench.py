@@ -301,14 +301,22 @@ LABEL_FORMS = (("labels_seed", False, True), ("labels_seed_ext", True, True),
                ("labels_seed_ext_all_events", True, False))
 
 
+def every_candidate(weights):
+    """The same scorer with its gates open: every event and every seeding candidate scored
+    (the quality operating point: most ghosts pruned, at a throughput cost)."""
+    from cuda_hlt_b200 import mlp
+    return mlp.dict_to_weights({**mlp.weights_to_dict(weights), "min_pairs": 0, "min_event_clusters": 0})
+
+
 def run_quality(weights, n, threads, label_events=2 * SIDE_BATCH):
     """Long-track efficiency and ghost rate of both forms against generator truth on the
     first n events of the workload (with MC truth), and of the label-pruned forms on the first
     label_events of them (their tracks equal the plain ones by construction; the GPU tests
     check it event by event). Events above the scorer's trained occupancy run the plain search
     in the pruned form; their number in the sample is reported."""
-    rows = {"plain": [], "pruned": []}
+    rows = {"plain": [], "pruned": [], "pruned_every_candidate": []}
     rows.update({name: [] for name, _, _ in LABEL_FORMS})
+    weights_all = every_candidate(weights)
     fallback = 0
 
     def add(name, b, res):
@@ -329,6 +337,11 @@ def run_quality(weights, n, threads, label_events=2 * SIDE_BATCH):
             add(name, b, res)
             if mode == chain.MODE_PRUNED:
                 fallback += int(((res["status"] & chain.STATUS["mlp_fallback"]) != 0).sum())
+        vc.set_mlp(weights_all)
+        vc.run_host(b)
+        vc.sync()
+        add("pruned_every_candidate", b, vc.results(clusters=False))
+        vc.set_mlp(weights)
         if a < label_events:
             for name, ext, fb in LABEL_FORMS:
                 vc.set_mode(chain.MODE_PLAIN)
@@ -351,6 +364,8 @@ def run_quality(weights, n, threads, label_events=2 * SIDE_BATCH):
     out["fallback_events"] = fallback
     out["long_efficiency_loss"] = out["plain"]["long_efficiency"] - out["pruned"]["long_efficiency"]
     out["ghost_rate_change"] = out["pruned"]["ghost_rate"] - out["plain"]["ghost_rate"]
+    out["every_candidate_long_efficiency_loss"] = (out["plain"]["long_efficiency"]
+                                                   - out["pruned_every_candidate"]["long_efficiency"])
     return out
 
 
@@ -444,11 +459,15 @@ def run_ours(args, rank, world, local_rank):
 
     forms = {}
     streams = [torch.cuda.Stream(device=dev) for _ in range(args.streams)]
-    for name, mode in (("plain", chain.MODE_PLAIN), ("pruned", chain.MODE_PRUNED)):
+    form_list = (("plain", chain.MODE_PLAIN, weights), ("pruned", chain.MODE_PRUNED, weights),
+                 ("pruned_every_candidate", chain.MODE_PRUNED, every_candidate(weights)))
+    for name, mode, form_weights in form_list:
+        if name == "pruned_every_candidate" and args.no_operating_points:
+            continue
         vcs = [chain.VeloChain(max_events=BUCKET, max_raw_bytes=max_batch_bytes + 4096, device=local_rank,
                                use_graphs=True) for _ in range(args.streams)]
         for vc in vcs:
-            vc.set_mlp(weights)
+            vc.set_mlp(form_weights)
             vc.set_mode(mode)
             vc.set_timing(True)  # before any graph capture: every graph then records its stage events
         vc = vcs[0]
@@ -537,6 +556,7 @@ def run_ours(args, rank, world, local_rank):
                   "search_mapping": q["search_mapping"], "decode_block": q["decode_block"],
                   "gpu_launches": q["gpu_launches"]},
         "pruned_vs_plain": p["value"] / q["value"],
+        "operating_points": operating_points(forms, quality),
         "quality": quality,
         "pruning_ceiling": ceiling,
         "e2e": e2e,
@@ -585,6 +605,24 @@ def link_bound(n_events, h2d_bytes, d2h_bytes, link):
     rest_rate = link["h2d_GBps"] if h2d_bytes > d2h_bytes else link["d2h_GBps"]
     rest = abs(h2d_bytes - d2h_bytes) / (rest_rate * 1e9)
     return n_events / (both + rest)
+
+
+def operating_points(forms, quality):
+    """The scorer at its committed gates (the bench's `value`) and with every candidate scored,
+    side by side: events/s against the plain chain, and the track quality of each."""
+    out = {}
+    for name, form in (("committed_gates", "pruned"), ("every_candidate", "pruned_every_candidate")):
+        if form not in forms:
+            continue
+        f = forms[form]
+        row = {"value": f["value"], "ms_per_step": f["ms_per_step"], "vs_plain": f["value"] / forms["plain"]["value"],
+               "stages_ms_per_batch_serial": f["stages_ms_per_batch_serial"]}
+        if quality:
+            qf = quality["pruned" if form == "pruned" else "pruned_every_candidate"]
+            row.update(long_efficiency_loss=quality["plain"]["long_efficiency"] - qf["long_efficiency"],
+                       ghost_rate=qf["ghost_rate"], plain_ghost_rate=quality["plain"]["ghost_rate"])
+        out[name] = row
+    return out
 
 
 def run_e2e(args, chunks, plan, local_rank, torch, world, dist, threshold, weights, decode_warps=8):
@@ -968,6 +1006,8 @@ def main():
     ap.add_argument("--no-ceiling", action="store_true", help="skip the per-stage / pruning-ceiling leg")
     ap.add_argument("--e2e-contexts", type=int, default=E2E_CONTEXTS,
                     help="contexts (and streams) in rotation in the end-to-end leg")
+    ap.add_argument("--no-operating-points", action="store_true",
+                    help="skip the timed form that scores every candidate")
     ap.add_argument("--e2e-depth", type=int, default=1,
                     help="end-to-end leg: batches launched before the oldest is read back (< contexts)")
     ap.add_argument("--batched-events", type=int, default=500_000,
