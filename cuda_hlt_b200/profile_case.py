@@ -3,11 +3,13 @@
 graphs, default output capacities: 400 tracks per event).
 
 python -m cuda_hlt_b200.profile_case [--events 8192] [--runs 2] [--block-threshold N] [--mode plain|pruned] [--pv]
-                                     [--gec]
+                                     [--gec] [--every-candidate]
 
 --block-threshold: events with more clusters than N use the block-per-event search, the
 others the warp-per-event one (1536 is the context default; 16384 sends every event to
 the warp search).
+--every-candidate: in the pruned mode, the committed scorer with its gates open (every event
+and every seeding candidate scored).
 """
 import argparse
 
@@ -22,6 +24,8 @@ def main():
     ap.add_argument("--block-threshold", type=int, default=1536)
     ap.add_argument("--mode", default="plain", choices=["plain", "pruned"])
     ap.add_argument("--pv", action="store_true", help="append the beamline PV stage")
+    ap.add_argument("--every-candidate", action="store_true",
+                    help="pruned mode: score every event and every seeding candidate")
     ap.add_argument("--gec", action="store_true",
                     help="global event cut in front of the chain, on synthetic UT / SciFi events (seed 0)")
     args = ap.parse_args()
@@ -40,7 +44,11 @@ def main():
     vc.set_pv(args.pv)
     if args.mode == "pruned":
         from cuda_hlt_b200 import mlp, train_scorer
-        vc.set_mlp(mlp.load_weights(train_scorer.DEFAULT_WEIGHTS))
+        w = mlp.load_weights(train_scorer.DEFAULT_WEIGHTS)
+        if args.every_candidate:
+            w.min_pairs = 0
+            w.min_event_clusters = 0
+        vc.set_mlp(w)
         vc.set_mode(chain.MODE_PRUNED)
     s = torch.cuda.current_stream().cuda_stream
     for _ in range(args.runs):
