@@ -524,6 +524,17 @@ def run_ours(args, rank, world, local_rank):
     # ---- end to end through velo_run_host with host buffers (pruned form) ----
     e2e = run_e2e(args, chunks, plan, local_rank, torch, world, dist, forms["pruned"]["threshold"], weights,
                    forms["pruned"]["decode_warps"])
+    # the same leg for the plain chain and for the scorer with every candidate scored: through
+    # host buffers the link bounds the rate, and pruned ghosts are bytes not read back
+    if not args.no_operating_points:
+        e2e["by_form"] = {"committed_gates": {"value": e2e["value"], "d2h_bytes_per_step": e2e["d2h_bytes_per_step"]}}
+        for name, mode, w in (("plain", chain.MODE_PLAIN, weights),
+                              ("every_candidate", chain.MODE_PRUNED, every_candidate(weights))):
+            r = run_e2e(args, chunks, plan, local_rank, torch, world, dist, forms["pruned"]["threshold"], w,
+                        forms["pruned"]["decode_warps"], mode=mode)
+            e2e["by_form"][name] = {"value": r["value"], "d2h_bytes_per_step": r["d2h_bytes_per_step"]}
+        for row in e2e["by_form"].values():
+            row["vs_plain"] = row["value"] / e2e["by_form"]["plain"]["value"]
 
     p, q = forms["pruned"], forms["plain"]
     result = {
@@ -625,7 +636,8 @@ def operating_points(forms, quality):
     return out
 
 
-def run_e2e(args, chunks, plan, local_rank, torch, world, dist, threshold, weights, decode_warps=8):
+def run_e2e(args, chunks, plan, local_rank, torch, world, dist, threshold, weights, decode_warps=8,
+            mode=None):
     """velo_run_host from pinned memory, E2E_CONTEXTS contexts in rotation, each on its own
     stream, so that the upload of one batch, the kernels of the next and the read-back of a
     third overlap (uploads and read-backs use the host link in opposite directions); outputs
@@ -646,7 +658,7 @@ def run_e2e(args, chunks, plan, local_rank, torch, world, dist, threshold, weigh
         vc.set_block_threshold(threshold)
         vc.set_decode_warps(decode_warps)
         vc.set_mlp(weights)
-        vc.set_mode(chain.MODE_PRUNED)
+        vc.set_mode(chain.MODE_PRUNED if mode is None else mode)
     streams = [torch.cuda.Stream(device=local_rank) for _ in range(nctx)]
     # pinned result buffers per context: atomics, hit numbers, hits SoA, Kalman states
     # (the workload averages 166 tracks and 1,340 track hits per event; a batch beyond these
