@@ -195,9 +195,11 @@ __device__ __forceinline__ bool umma_wait(uint64_t* mbar, uint32_t& phase)
 }
 
 // ---------------------------------------------------------------------------------
-// Inference on 128-row tiles (128 threads, one row each)
+// Inference on 128-row tiles (128 threads, one row each): the trainer's row inference. The
+// chain's scorer (score_candidates_kernel) runs two tiles per CTA with all three layers on
+// the tensor core instead.
 // ---------------------------------------------------------------------------------
-// Inference keeps the hidden layer at K = 64 (the layer-2 bias is added in fp32 in the
+// This inference keeps the hidden layer at K = 64 (the layer-2 bias is added in fp32 in the
 // epilogue: the same bf16 value the training's ones column multiplies by 1) and computes the
 // two-output head on the CUDA cores, so it needs neither the padded H columns nor a W3 tile.
 struct __align__(128) MlpInferSmem {
