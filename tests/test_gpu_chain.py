@@ -388,6 +388,56 @@ def test_host_offsets_staging():
     vc.close()
 
 
+def test_contexts_on_threads():
+    """Separate contexts run concurrently: two host threads, each with its own context and
+    stream (as Allen runs one Stream per thread), repeat their own batch (one in the plain
+    mode, one pruned) while the other runs; every result equals the same batch run alone."""
+    import threading
+
+    import torch
+    from cuda_hlt_b200 import mlp, train_scorer
+    w = mlp.load_weights(train_scorer.DEFAULT_WEIGHTS)
+    jobs = [(events.generate_config("batched_500k", n_events=200, first_event=900), chain.MODE_PLAIN),
+            (events.generate_config("pruned_1m", n_events=200, first_event=30_000), chain.MODE_PRUNED)]
+    alone = []
+    for b, mode in jobs:
+        vc = chain.VeloChain(max_events=b.n_events, max_raw_bytes=int(b.raw.size) + 4096)
+        vc.set_mlp(w)
+        vc.set_mode(mode)
+        vc.run_host(b)
+        vc.sync()
+        alone.append(vc.results())
+        vc.close()
+    got = [[] for _ in jobs]
+    errors = []
+
+    def worker(i):
+        try:
+            b, mode = jobs[i]
+            stream = torch.cuda.Stream()
+            vc = chain.VeloChain(max_events=b.n_events, max_raw_bytes=int(b.raw.size) + 4096, use_graphs=True)
+            vc.set_mlp(w)
+            vc.set_mode(mode)
+            for _ in range(4):
+                vc.run_host(b, stream.cuda_stream)
+                vc.sync()
+                got[i].append(vc.results())
+            vc.close()
+        except Exception as ex:  # reported by the main thread
+            errors.append((i, ex))
+
+    threads = [threading.Thread(target=worker, args=(i,)) for i in range(len(jobs))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors
+    for i, (b, _) in enumerate(jobs):
+        assert len(got[i]) == 4
+        for k, res in enumerate(got[i]):
+            _same_results(alone[i], res, b.n_events, f"thread {i}, run {k}")
+
+
 def test_selected_events_u32():
     """velo_run_selected_u32 decodes the caller's selection (Allen's dev_event_list after
     global_event_cut_t): position i holds raw event list[i], equal to a run over those events
