@@ -308,6 +308,23 @@ def test_trained_scorer_prunes_at_no_efficiency_cost():
     assert st_pruned["search_by_triplet"] < 0.95 * st_plain["search_by_triplet"]
 
 
+def test_committed_scorer_with_every_candidate_scored():
+    """The committed scorer with its gates open (every event and every seeding candidate
+    scored: the quality operating point the bench reports) on events of the bench workload
+    (nu ~ U(2,20)) with MC truth: long-track efficiency within 0.2% absolute of the plain
+    search, and most ghosts gone."""
+    from cuda_hlt_b200 import train_scorer
+    w = mlp.load_weights(train_scorer.DEFAULT_WEIGHTS)
+    w.min_pairs = 0
+    w.min_event_clusters = 0
+    ev = events.generate_config("pruned_1m", n_events=4096, first_event=100_000, threads=8, with_mc=True)
+    plain = run_mode(ev, chain.MODE_PLAIN)
+    pruned = run_mode(ev, chain.MODE_PRUNED, w)
+    cp, cq = chain.check_tracks(ev, plain), chain.check_tracks(ev, pruned)
+    assert cq.long_efficiency >= cp.long_efficiency - 0.002, (cp.long_efficiency, cq.long_efficiency)
+    assert cq.ghost_rate < 0.5 * cp.ghost_rate, (cp.ghost_rate, cq.ghost_rate)
+
+
 def test_label_mode_is_the_pruning_ceiling():
     """VELO_MODE_LABELS prunes with the plain search's own labels of the same batch (a perfect
     scorer at no cost). Every final track of the plain search - ghosts included - is made of
