@@ -666,12 +666,22 @@ __global__ void __launch_bounds__(W * 32, 40 / W) decode_cluster_sort_kernel(Cha
           const bool fallback = nh > P.mlp.max_hits;  // above the trained occupancy: plain search
           if (fallback && threadIdx.x == 0) sh.flags |= kStatusMlpFallback;
           score = !fallback && nh >= P.mlp.min_hits;
-          // modules 0, 1, 50, 51 hold no h1: extension candidates only
-          for (uint32_t h = threadIdx.x; h < sh.mod_start[2]; h += blockDim.x) K[h] = 2;
-          for (uint32_t h = sh.mod_start[50] + threadIdx.x; h < nh; h += blockDim.x) K[h] = 2;
+          if (score) {
+            // modules 0, 1, 50, 51 hold no h1: extension candidates only
+            for (uint32_t h = threadIdx.x; h < sh.mod_start[2]; h += blockDim.x) K[h] = 2;
+            for (uint32_t h = sh.mod_start[50] + threadIdx.x; h < nh; h += blockDim.x) K[h] = 2;
+          } else {
+            // an event the scorer does not score: every seed kept, its windows as in the
+            // plain mode (the branch is uniform over the block)
+            for (uint32_t h = threadIdx.x; h < nh; h += blockDim.x) K[h] = 3;
+          }
         }
-        for (uint32_t m = 2 + warp; m < 50; m += W)
-          module_windows<kPruned>(P, sphi, H, P.windows + base, K, base, m, sh.mod_start, sh.mod_count, score);
+        if (kPruned && score)
+          for (uint32_t m = 2 + warp; m < 50; m += W)
+            module_windows<true>(P, sphi, H, P.windows + base, K, base, m, sh.mod_start, sh.mod_count, true);
+        else
+          for (uint32_t m = 2 + warp; m < 50; m += W)
+            module_windows<false>(P, sphi, H, P.windows + base, K, base, m, sh.mod_start, sh.mod_count, false);
       }
     }
     __syncthreads();

@@ -190,7 +190,9 @@ typedef struct VeloConfig {
  *   module_hit_start[N*52], module_hit_num[N*52] (starts are absolute indices; gaps allowed),
  *   hit_xyzp (4 floats per cluster: x, y, z, phi) and hit_id indexed by those starts,
  *   hit_size (pixels of each cluster, at most 3) and, in VELO_MODE_PRUNED, hit_keep (the
- *   scorer's bits per hit: bit 0 seed keep, bit 1 extension keep; NULL in the plain mode). */
+ *   scorer's bits per hit: bit 0 seed keep, bit 1 extension keep; both set on every hit of an
+ *   event the scorer does not score, below its event gate or above its trained occupancy;
+ *   NULL in the plain mode). */
 typedef struct VeloOutputs {
   uint32_t n_events;
   uint32_t* atomics;
