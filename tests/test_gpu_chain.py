@@ -388,6 +388,36 @@ def test_host_offsets_staging():
     vc.close()
 
 
+def test_context_memory_released():
+    """velo_destroy returns what velo_create and the runs took (device buffers, the pruned
+    mode's buffers allocated on first use, CUDA graphs per batch-size bucket): free device
+    memory after five create / run / destroy cycles equals free memory before them, to within
+    what the CUDA runtime itself keeps."""
+    import torch
+    from cuda_hlt_b200 import mlp, train_scorer
+    w = mlp.load_weights(train_scorer.DEFAULT_WEIGHTS)
+    b = events.generate_config("pruned_1m", n_events=1500, first_event=40_000)
+    torch.cuda.synchronize()
+
+    def cycle():
+        vc = chain.VeloChain(max_events=4096, max_raw_bytes=int(b.raw.size) + 4096, use_graphs=True)
+        vc.set_mlp(w)
+        for mode in (chain.MODE_PLAIN, chain.MODE_PRUNED):
+            vc.set_mode(mode)
+            vc.run_host(b)
+            vc.run_host(b.subset(0, 1000))
+            vc.sync()
+        assert vc.graph_count() >= 1
+        vc.close()
+
+    cycle()  # first use: the runtime's own lazy allocations happen here
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(5):
+        cycle()
+    free1 = torch.cuda.mem_get_info()[0]
+    assert free0 - free1 < 64 << 20, (free0, free1)
+
+
 def test_contexts_on_threads():
     """Separate contexts run concurrently: two host threads, each with its own context and
     stream (as Allen runs one Stream per thread), repeat their own batch (one in the plain
