@@ -50,7 +50,7 @@ N_EVENTS = 1_000_000
 BUCKET = 65536   # events per batch (one CUDA graph); --batch
 CHUNK = 4 * BUCKET
 SIDE_BATCH = 16384  # batches of the MC-quality and reference-kernel legs
-E2E_CONTEXTS = 3    # contexts (and streams) in rotation in the end-to-end leg
+E2E_CONTEXTS = 4    # contexts (and streams) in rotation in the end-to-end leg
 
 
 def log(*a):
@@ -521,6 +521,11 @@ def run_ours(args, rank, world, local_rank):
         ceiling = pruning_ceiling(weights, batch_ptrs, max_batch_bytes, forms["plain"]["threshold"],
                                   forms["plain"]["decode_warps"], stream, torch)
 
+    # the device-resident copy of the workload is done with: the end-to-end leg reads host
+    # buffers, and its contexts need the room
+    del batch_ptrs, d_offs, d_raw
+    torch.cuda.empty_cache()
+
     # ---- end to end through velo_run_host with host buffers (pruned form) ----
     e2e = run_e2e(args, chunks, plan, local_rank, torch, world, dist, forms["pruned"]["threshold"], weights,
                    forms["pruned"]["decode_warps"])
@@ -577,9 +582,10 @@ def run_ours(args, rank, world, local_rank):
     return result, chunks
 
 
-def host_link(torch, local_rank, nbytes=1 << 30, chunk=64 << 20, reps=3):
+def host_link(torch, local_rank, nbytes=2 << 30, chunk=64 << 20, reps=5):
     """Copy rates of this GPU's host link in GB/s: pinned host to device and device to host,
-    each alone and both at once (one stream per direction, 64 MB copies)."""
+    each alone and both at once (one stream per direction, 64 MB copies); the best of `reps`
+    passes of `nbytes` each (a single pass can land on a slow moment of a shared host)."""
     dev = torch.device("cuda", local_rank)
     h_up = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
     h_down = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
@@ -596,12 +602,14 @@ def host_link(torch, local_rank, nbytes=1 << 30, chunk=64 << 20, reps=3):
         for job in jobs:
             copies(*job)
         torch.cuda.synchronize(dev)
-        t0 = time.perf_counter()
+        best = 0.0
         for _ in range(reps):
+            t0 = time.perf_counter()
             for job in jobs:
                 copies(*job)
-        torch.cuda.synchronize(dev)
-        return nbytes * reps / (time.perf_counter() - t0) / 1e9
+            torch.cuda.synchronize(dev)
+            best = max(best, nbytes / (time.perf_counter() - t0) / 1e9)
+        return best
 
     up, down = (d_up, h_up, s_up), (h_down, d_down, s_down)
     out = {"h2d_GBps": rate(up), "d2h_GBps": rate(down), "both_GBps_each_direction": rate(up, down)}
@@ -651,14 +659,24 @@ def run_e2e(args, chunks, plan, local_rank, torch, world, dist, threshold, weigh
         o = chunks[ci].offsets[a:b + 1]
         offs.append(np.ascontiguousarray(o - o[0], dtype=np.uint64))
     max_batch_bytes = max(int(chunks[ci].offsets[b] - chunks[ci].offsets[a]) for ci, a, b in plan)
-    nctx = args.e2e_contexts
-    ctxs = [chain.VeloChain(max_events=BUCKET, max_raw_bytes=max_batch_bytes + 4096, device=local_rank)
-            for _ in range(nctx)]
-    for vc in ctxs:
-        vc.set_block_threshold(threshold)
-        vc.set_decode_warps(decode_warps)
-        vc.set_mlp(weights)
-        vc.set_mode(chain.MODE_PRUNED if mode is None else mode)
+    # as many contexts as asked for and the device holds (at least two)
+    ctxs = []
+    for _ in range(args.e2e_contexts):
+        vc = None
+        try:
+            vc = chain.VeloChain(max_events=BUCKET, max_raw_bytes=max_batch_bytes + 4096, device=local_rank)
+            vc.set_block_threshold(threshold)
+            vc.set_decode_warps(decode_warps)
+            vc.set_mlp(weights)
+            vc.set_mode(chain.MODE_PRUNED if mode is None else mode)
+            ctxs.append(vc)
+        except chain.VeloError:
+            if vc is not None:
+                vc.close()
+            if len(ctxs) < 2:
+                raise
+            break
+    nctx = len(ctxs)
     streams = [torch.cuda.Stream(device=local_rank) for _ in range(nctx)]
     # pinned result buffers per context: atomics, hit numbers, hits SoA, Kalman states
     # (the workload averages 166 tracks and 1,340 track hits per event; a batch beyond these
