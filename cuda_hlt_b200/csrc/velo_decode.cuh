@@ -676,10 +676,15 @@ __global__ void __launch_bounds__(W * 32, 40 / W) decode_cluster_sort_kernel(Cha
             for (uint32_t h = threadIdx.x; h < nh; h += blockDim.x) K[h] = 3;
           }
         }
-        if (kPruned && score)
-          for (uint32_t m = 2 + warp; m < 50; m += W)
-            module_windows<true>(P, sphi, H, P.windows + base, K, base, m, sh.mod_start, sh.mod_count, true);
-        else
+        bool scored = false;
+        if constexpr (kPruned) {
+          if (score) {
+            for (uint32_t m = 2 + warp; m < 50; m += W)
+              module_windows<true>(P, sphi, H, P.windows + base, K, base, m, sh.mod_start, sh.mod_count, true);
+            scored = true;
+          }
+        }
+        if (!scored)
           for (uint32_t m = 2 + warp; m < 50; m += W)
             module_windows<false>(P, sphi, H, P.windows + base, K, base, m, sh.mod_start, sh.mod_count, false);
       }
