@@ -45,33 +45,33 @@ __global__ void __launch_bounds__(kFillThreads) candidate_features_kernel(ChainP
   }
 }
 
-// score_candidates: 256 threads, two 128-row tiles per iteration. Warps 0-3 hold the rows of
-// the first tile, warps 4-7 those of the second (a warp reads the TMEM lanes 32 * (warp % 4)
-// onwards, so both halves read their own tile's accumulators, 64 columns apart): one barrier
-// round and one tensor-core round trip per layer serve two tiles. All three layers run on
-// the tensor core, in the training kernel's layouts: hidden tiles 80 wide with a ones column,
-// so the layer-2 and head biases come out of the MMAs, and each epilogue is ReLU, round to
-// bf16 and store; the logits are the first two columns of the head's accumulators. Tile
-// pairs are bulk-copied (8 KB, contiguous in the candidate list) into a two-deep ring, one
-// pair ahead; the epilogues take their accumulators 16 columns at a time, so three CTAs fit
-// on an SM without spilling.
-constexpr uint32_t kScorePair = 2;                                  // tiles per iteration
+// score_candidates: 256 threads in two independent halves of 128 that share the weights in
+// shared memory and one tensor-memory allocation. Half h (warps 4h .. 4h + 3; a warp reads
+// the TMEM lanes 32 * (warp % 4) onwards) scores its own stream of 128-row tiles with its own
+// 64 TMEM columns, load ring, MMA barrier and named barrier (1 + h), so one half runs its
+// epilogues while the other waits on the tensor core. All three layers run on the tensor
+// core, in the training kernel's layouts: hidden tiles 80 wide with a ones column, so the
+// layer-2 and head biases come out of the MMAs, and each epilogue is ReLU, round to bf16 and
+// store; the logits are the first two columns of the head's accumulators. Tiles are
+// bulk-copied into a two-deep ring per half, one tile ahead; the epilogues take their
+// accumulators 16 columns at a time, so three CTAs fit on an SM without spilling.
+constexpr uint32_t kScorePair = 2;                                  // halves per CTA
 constexpr uint32_t kScoreThreads = kMlpTile * kScorePair;           // 256
-constexpr uint32_t kScoreRing = 2;                                  // tile pairs in the ring
+constexpr uint32_t kScoreRing = 2;                                  // tiles in a half's ring
 constexpr uint32_t kScoreTmemCols = kMlpHidden * kScorePair;        // 128
 struct __align__(128) ScoreSmem {
   uint8_t w1[kMlpW1 * 2];                          // W1 [64][16]
   uint8_t w2[kMlpW2 * 2];                          // W2 [64][80], bias in column 64
   uint8_t w3[kMlpW3 * 2];                          // W3 [16][80], rows 2..15 zero
-  uint8_t x[kScoreRing][kScorePair * kCandTileBytes];
+  uint8_t x[kScorePair][kScoreRing][kCandTileBytes];
   uint8_t h[kScorePair][kMlpTile * kMlpK2 * 2];    // H1, then H2: [128][80], 1.0 in column 64
-  uint64_t load_bar[kScoreRing];
-  uint64_t mbar;
+  uint64_t load_bar[kScorePair][kScoreRing];
+  uint64_t mbar[kScorePair];
   uint32_t tmem;
 };
 constexpr uint32_t kScoreSmem = sizeof(ScoreSmem) + 128;
 
-// This thread's row of a tile pair: half (0/1) picks the tile, row its row in it.
+// This thread's half (0/1) and its row in the half's tile.
 __device__ __forceinline__ uint32_t score_half() { return threadIdx.x >> 7; }
 __device__ __forceinline__ uint32_t score_row() { return threadIdx.x & (kMlpTile - 1); }
 
@@ -96,18 +96,52 @@ __device__ __forceinline__ void score_hidden_epilogue(uint8_t* h, uint32_t taddr
   }
 }
 
-// One layer on both tiles of the pair: D(half j) = A_j * B^T into TMEM columns 64 j.., then
-// wait. False (uniformly) on timeout.
-__device__ __forceinline__ bool score_layer(ScoreSmem& s, uint32_t& phase, const uint8_t* a0, const uint8_t* a1,
+// Named barrier of one half (barrier 1 + half, its 128 threads); the ids are immediates, so
+// the kernel holds three barriers (the half is the same for all threads of a half).
+__device__ __forceinline__ void half_sync(uint32_t half)
+{
+  if (half == 0) asm volatile("bar.sync 1, 128;" ::: "memory");
+  else asm volatile("bar.sync 2, 128;" ::: "memory");
+}
+
+// AND of `v` over the threads of one half, at its named barrier.
+__device__ __forceinline__ bool half_and(uint32_t half, bool v)
+{
+  uint32_t r;
+  if (half == 0)
+    asm volatile(
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.and.pred q, 1, 128, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(r)
+      : "r"(v ? 1u : 0u)
+      : "memory");
+  else
+    asm volatile(
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.and.pred q, 2, 128, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(r)
+      : "r"(v ? 1u : 0u)
+      : "memory");
+  return r != 0;
+}
+
+// One layer on this half's tile: D = A * B^T into the half's 64 TMEM columns, then wait.
+// False (uniformly over the half) on timeout.
+__device__ __forceinline__ bool score_layer(ScoreSmem& s, uint32_t half, uint32_t& phase, const uint8_t* a,
                                             uint32_t a_sbo, const uint8_t* b, uint32_t b_sbo, uint32_t k, uint32_t n)
 {
-  umma_stage_barrier();
-  if (threadIdx.x == 0) {
-    umma_issue(s.tmem, a0, a_sbo, b, b_sbo, k, n, false);
-    umma_issue(s.tmem + kMlpHidden, a1, a_sbo, b, b_sbo, k, n, false);
-    umma_commit(&s.mbar);
+  fence_async_smem();  // this half's shared-memory writes, visible to the tensor core
+  tc_fence_before();
+  half_sync(half);
+  tc_fence_after();
+  if (score_row() == 0) {
+    umma_issue(s.tmem + half * kMlpHidden, a, a_sbo, b, b_sbo, k, n, false);
+    umma_commit(&s.mbar[half]);
   }
-  return umma_wait(&s.mbar, phase);
+  const bool ok = mbar_wait_parity(&s.mbar[half], phase);
+  phase ^= 1u;
+  tc_fence_after();
+  return half_and(half, ok);
 }
 
 __global__ void __launch_bounds__(kScoreThreads, 3) score_candidates_kernel(ChainPointers P)
@@ -116,14 +150,14 @@ __global__ void __launch_bounds__(kScoreThreads, 3) score_candidates_kernel(Chai
   ScoreSmem& s = *reinterpret_cast<ScoreSmem*>((reinterpret_cast<uintptr_t>(s_dyn) + 127) & ~uintptr_t(127));
   const uint32_t rows = P.queue[7];
   const uint32_t tiles = (rows + kMlpTile - 1) / kMlpTile;
-  const uint32_t pairs = (tiles + kScorePair - 1) / kScorePair;
-  if (blockIdx.x >= pairs) return;  // uniform: this CTA has no tile
-  // set-up: tensor memory, barriers, weights (as mlp_infer_setup, for the pair layout)
+  if (blockIdx.x * kScorePair >= tiles) return;  // uniform: neither half has a tile
+  // set-up: tensor memory, barriers, weights (as mlp_infer_setup, for the three-layer layout)
   if (threadIdx.x < 32) tmem_alloc(&s.tmem, kScoreTmemCols);
-  if (threadIdx.x == 0) {
-    mbar_init1(&s.mbar);
-    for (uint32_t i = 0; i < kScoreRing; ++i) mbar_init1(&s.load_bar[i]);
-  }
+  if (threadIdx.x == 0)
+    for (uint32_t h = 0; h < kScorePair; ++h) {
+      mbar_init1(&s.mbar[h]);
+      for (uint32_t i = 0; i < kScoreRing; ++i) mbar_init1(&s.load_bar[h][i]);
+    }
   load_canon(s.w1, P.mlp.w, kMlpHidden, kMlpK1);
   load_canon(s.w2, P.mlp.w + kMlpW1, kMlpHidden, kMlpK2);
   load_canon(s.w3, P.mlp.w + kMlpW1 + kMlpW2, kMlpOutPad, kMlpK2);
@@ -135,48 +169,46 @@ __global__ void __launch_bounds__(kScoreThreads, 3) score_candidates_kernel(Chai
   }
   umma_stage_barrier();  // publishes the barrier inits, the weights and the TMEM address
 
-  // pair p (tiles 2p, 2p + 1) is 8 KB at tile 2p; the last pair may hold one tile
-  auto issue_load = [&](uint32_t pair, uint32_t slot) {
-    const uint32_t t0 = pair * kScorePair;
-    const uint32_t n = min(kScorePair, tiles - t0);
-    bulk_load_smem(s.x[slot], P.cand_feat + static_cast<size_t>(t0) * kCandTileBytes, n * kCandTileBytes,
-                   &s.load_bar[slot]);
+  const uint32_t half = score_half(), row = score_row();
+  const uint32_t taddr_row = s.tmem + (((threadIdx.x >> 5) & 3u) * 32u << 16) + half * kMlpHidden;
+  // this half's tiles: first, first + workers, ...; its k-th tile goes to ring slot k % ring
+  const uint32_t workers = kScorePair * gridDim.x, first = kScorePair * blockIdx.x + half;
+  auto issue_load = [&](uint32_t t, uint32_t slot) {
+    bulk_load_smem(s.x[half][slot], P.cand_feat + static_cast<size_t>(t) * kCandTileBytes, kCandTileBytes,
+                   &s.load_bar[half][slot]);
   };
   uint32_t mma_phase = 0, load_phase = 0;  // load_phase: bit i = parity of slot i
   bool ok = true;
-  // this CTA's pairs are blockIdx.x + k * gridDim.x; pair k goes to slot k % ring
-  if (threadIdx.x == 0)
+  if (row == 0)
     for (uint32_t k = 0; k + 1 < kScoreRing; ++k) {
-      const uint32_t p = blockIdx.x + k * gridDim.x;
-      if (p < pairs) issue_load(p, k);
+      const uint32_t t = first + k * workers;
+      if (t < tiles) issue_load(t, k);
     }
-  const uint32_t half = score_half(), row = score_row();
-  const uint32_t taddr_row = s.tmem + (((threadIdx.x >> 5) & 3u) * 32u << 16) + half * kMlpHidden;
   uint32_t k = 0;
-  for (uint32_t pair = blockIdx.x; pair < pairs; pair += gridDim.x, ++k) {
+  for (uint32_t t = first; t < tiles; t += workers, ++k) {
     const uint32_t slot = k % kScoreRing;
-    // refill the slot that pair k - 1 used (its MMAs are complete) with pair k + ring - 1
-    const uint32_t ahead = pair + (kScoreRing - 1) * gridDim.x;
-    if (threadIdx.x == 0 && ahead < pairs) issue_load(ahead, (k + kScoreRing - 1) % kScoreRing);
-    const uint32_t r = (pair * kScorePair + half) * kMlpTile + row;
+    // refill the slot that tile k - 1 used (its MMAs are complete) with tile k + ring - 1
+    const uint32_t ahead = t + (kScoreRing - 1) * workers;
+    if (row == 0 && ahead < tiles) issue_load(ahead, (k + kScoreRing - 1) % kScoreRing);
+    const uint32_t r = t * kMlpTile + row;
     const uint32_t hit = r < rows ? P.cand_slot[r] : 0u;  // issued early: used after the MMAs
-    const bool loaded = mbar_wait_parity(&s.load_bar[slot], (load_phase >> slot) & 1u);
+    const bool loaded = mbar_wait_parity(&s.load_bar[half][slot], (load_phase >> slot) & 1u);
     load_phase ^= 1u << slot;
-    if (!__syncthreads_and(loaded)) {
+    if (!half_and(half, loaded)) {
       ok = false;
       break;
     }
-    if (!score_layer(s, mma_phase, s.x[slot], s.x[slot] + kCandTileBytes, kSbo1, s.w1, kSbo1, kMlpK1, kMlpHidden)) {
+    if (!score_layer(s, half, mma_phase, s.x[half][slot], kSbo1, s.w1, kSbo1, kMlpK1, kMlpHidden)) {
       ok = false;
       break;
     }
     score_hidden_epilogue(s.h[half], taddr_row, row);  // H1
-    if (!score_layer(s, mma_phase, s.h[0], s.h[1], kSbo2, s.w2, kSbo2, kMlpK2, kMlpHidden)) {
+    if (!score_layer(s, half, mma_phase, s.h[half], kSbo2, s.w2, kSbo2, kMlpK2, kMlpHidden)) {
       ok = false;
       break;
     }
     score_hidden_epilogue(s.h[half], taddr_row, row);  // H2, over H1 (layer 2 has read it)
-    if (!score_layer(s, mma_phase, s.h[0], s.h[1], kSbo2, s.w3, kSbo2, kMlpK2, kMlpOutPad)) {
+    if (!score_layer(s, half, mma_phase, s.h[half], kSbo2, s.w3, kSbo2, kMlpK2, kMlpOutPad)) {
       ok = false;
       break;
     }
@@ -191,14 +223,14 @@ __global__ void __launch_bounds__(kScoreThreads, 3) score_candidates_kernel(Chai
       P.keep[hit] = static_cast<uint8_t>((seed ? 1u : 0u) | (ext ? 2u : 0u));
     }
   }
-  if (!ok && threadIdx.x == 0) {
+  if (!ok && row == 0) {
     atomicOr(P.queue + 6, kErrorMlpTimeout);
-    // copies still in flight must land before the CTA exits: wait (bounded) on every slot
-    // whose issued copy has not been consumed
-    for (uint32_t j = 0; j < kScoreRing; ++j) mbar_wait_parity(&s.load_bar[j], (load_phase >> j) & 1u);
+    // this half's copies still in flight must land before the CTA exits: wait (bounded) on
+    // every slot whose issued copy has not been consumed
+    for (uint32_t j = 0; j < kScoreRing; ++j) mbar_wait_parity(&s.load_bar[half][j], (load_phase >> j) & 1u);
   }
   tc_fence_before();
-  __syncthreads();
+  __syncthreads();  // both halves
   tc_fence_after();
   if (threadIdx.x < 32) tmem_dealloc(s.tmem, kScoreTmemCols);
 }
