@@ -44,3 +44,35 @@ def test_roofline_of_the_dominant_serial_stage():
     assert roof["frac"] == pytest.approx(roof["achieved"] / 1000.0)
     assert roof["serial_single_stream"]["avg_launch_ms"] == 3.0
     assert roof["serial_single_stream"]["achieved"] == pytest.approx(per["decode_cluster_sort"] / 3e-3 / 1e9)
+
+
+def test_every_candidate_opens_only_the_gates():
+    from cuda_hlt_b200 import mlp, train_scorer
+    w = mlp.load_weights(train_scorer.DEFAULT_WEIGHTS)
+    wa = bench.every_candidate(w)
+    a, b = mlp.weights_to_dict(w), mlp.weights_to_dict(wa)
+    assert b["min_pairs"] == 0 and b["min_event_clusters"] == 0
+    assert a["min_pairs"] > 0 and a["min_event_clusters"] > 0  # the committed gates are untouched
+    for k in ("mean", "inv_std", "w1", "w2", "w3"):
+        assert (a[k] == b[k]).all()
+    for k in ("seed_threshold", "ext_threshold", "max_event_clusters"):
+        assert a[k] == b[k]
+
+
+def test_operating_points_table():
+    serial = {"decode_cluster_sort": 1.0}
+    forms = {"plain": {"value": 100.0, "ms_per_step": 10.0, "stages_ms_per_batch_serial": serial},
+             "pruned": {"value": 99.0, "ms_per_step": 10.1, "stages_ms_per_batch_serial": serial},
+             "pruned_every_candidate": {"value": 86.0, "ms_per_step": 11.6, "stages_ms_per_batch_serial": serial}}
+    quality = {"plain": {"long_efficiency": 0.9868, "ghost_rate": 0.0648},
+               "pruned": {"long_efficiency": 0.9867, "ghost_rate": 0.0576},
+               "pruned_every_candidate": {"long_efficiency": 0.9861, "ghost_rate": 0.0142}}
+    op = bench.operating_points(forms, quality)
+    assert op["committed_gates"]["vs_plain"] == pytest.approx(0.99)
+    assert op["every_candidate"]["vs_plain"] == pytest.approx(0.86)
+    assert op["every_candidate"]["long_efficiency_loss"] == pytest.approx(0.0007)
+    assert op["every_candidate"]["ghost_rate"] == 0.0142 and op["every_candidate"]["plain_ghost_rate"] == 0.0648
+    # without the every-candidate form (--no-operating-points) and without a quality leg
+    del forms["pruned_every_candidate"]
+    op = bench.operating_points(forms, None)
+    assert list(op) == ["committed_gates"] and "ghost_rate" not in op["committed_gates"]
